@@ -1,0 +1,591 @@
+"""
+bench.py — the BN254 prover hot path on B200: large plain instances.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload large|small]
+
+Workload "large" (default; BASELINE.json's metric is quoted on it): one step =
+  MSM over 2^22 BN254 G1 points with uniform scalars
+  + the same MSM with skewed witness-like scalars (60% in {0,1}, 20% < 2^32)
+  + a forward Fr NTT of 2^24 elements
+  + a forward coset NTT (g = 5) of 2^24 elements.
+Inputs are seeded synthetic data with the configs' shapes (bases k_i G, k_i
+uniform in [1, r)); every input is larger than the 126 MB L2.
+
+Prints ONE JSON line (rank 0). `value` is device time per step with inputs
+resident in HBM (CUDA events, max over ranks); `e2e` is the same step through
+the public Python API from pinned host buffers, copies included; `roofline`
+covers the dominant kernel (the MSM bucket accumulation, integer-multiply
+bound) timed live with CUDA events recorded by the library on its stream;
+`cpu_baseline` is the oracle (a C port of the reference's CPU algorithms)
+timed on a bounded sample on one host core.
+
+--impl reference runs the reference's CPU algorithms (the same C port, all
+host threads) on the same workload and prints the same line with
+"impl": "reference".
+
+N > 1 (torchrun): every rank runs its own instance of the step (weak
+scaling, no collective on the data path); the time is the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "zk-gpu-accelerator_b200"))
+sys.path.insert(0, str(ROOT))
+
+METRIC = "MSM 2^22 / NTT 2^24 ms on 1 B200; batched jobs/s vs plain launches; p99 latency"
+UNIT = "ms"
+SCALAR_BITS = 254
+COSET = 5
+
+WORKLOADS = {
+    # name: (log2 MSM points, log2 NTT size)
+    "large": (22, 24),
+    "small": (18, 20),  # for profiler captures: a few GB on the device
+}
+
+
+def _peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text())
+        except ValueError:
+            pass
+    return {}
+
+
+# ------------------------------------------------------------------
+# Work accounting
+# ------------------------------------------------------------------
+
+IMAD_PER_MULMOD = 264  # 2 x 64 32-bit multiply-adds (lo and hi) for a*b and m*p, plus 8 for the m's
+MULMOD_PER_MADD = 10   # XYZZ mixed addition: 8 multiplications + 2 squarings
+
+
+def nonzero_digits(scalars, w: int) -> int:
+    """Nonzero signed w-bit digits over all windows: the pairs the bucket kernel adds
+    (same recoding as csrc/msm.cu: windows of w bits, digit > 2^(w-1) borrows)."""
+    import numpy as np
+
+    n = scalars.shape[0]
+    W = -(-(SCALAR_BITS + 1) // w)
+    half = 1 << (w - 1)
+    carry = np.zeros(n, dtype=np.int64)
+    total = 0
+    limbs = [scalars[:, j].astype(np.uint64) for j in range(4)]
+    for win in range(W):
+        lo = win * w
+        limb, off = lo // 64, lo % 64
+        if limb < 4:
+            v = limbs[limb] >> np.uint64(off)
+            if off + w > 64 and limb + 1 < 4:
+                v = v | (limbs[limb + 1] << np.uint64(64 - off))
+            raw = (v & np.uint64((1 << w) - 1)).astype(np.int64) + carry
+        else:
+            raw = carry.copy()
+        if win + 1 < W:
+            borrow = raw > half
+            mag = np.where(borrow, (1 << w) - raw, raw)
+            carry = borrow.astype(np.int64)
+        else:
+            mag = raw
+        total += int(np.count_nonzero(mag))
+    return total
+
+
+# ------------------------------------------------------------------
+# Clocks (nvidia-smi sampled during the timed region)
+# ------------------------------------------------------------------
+
+CLOCK_QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+
+class ClockSampler:
+    def __init__(self, gpu_index: int) -> None:
+        self.gpu = gpu_index
+        self.proc: subprocess.Popen | None = None
+        self.lines: list[str] = []
+        self._t: threading.Thread | None = None
+
+    def __enter__(self) -> ClockSampler:
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={CLOCK_QUERY}", "--format=csv,noheader,nounits", "-lms", "100",
+                 "-i", str(self.gpu)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True,
+            )
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def _read(self) -> None:
+        assert self.proc and self.proc.stdout
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc) -> None:
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self._t:
+            self._t.join(timeout=2)
+
+    def summary(self) -> dict:
+        rows = []
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append({"sm": float(parts[1]), "max": float(parts[2]), "power": float(parts[3]),
+                             "hw": parts[5], "hw_thermal": parts[6], "sw_thermal": parts[7], "sw_power": parts[8]})
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        loaded = [r for r in rows if r["power"] > 0.5 * max(r["power"] for r in rows)] or rows
+        reasons = []
+        for key, name in (("hw", "hw_slowdown"), ("hw_thermal", "hw_thermal_slowdown"),
+                          ("sw_thermal", "sw_thermal_slowdown"), ("sw_power", "sw_power_cap")):
+            if any(r[key].lower() == "active" for r in rows):
+                reasons.append(name)
+        return {"sm_mhz": statistics.median(r["sm"] for r in loaded), "sm_max_mhz": max(r["max"] for r in rows),
+                "reasons": reasons, "samples": len(rows), "power_w_max": max(r["power"] for r in rows)}
+
+
+# ------------------------------------------------------------------
+# Distributed plumbing
+# ------------------------------------------------------------------
+
+
+def dist_env() -> tuple[int, int, int]:
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def init_dist(world: int, backend: str):
+    if world <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=300))
+    return dist
+
+
+def max_over_ranks(value: float, dist, device) -> float:
+    """The largest value any rank reports (all ranks call this in the same order)."""
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist, device) -> None:
+    if dist is not None:
+        import torch
+
+        dist.barrier(device_ids=[device.index] if device is not None and device.type == "cuda" else None)
+
+
+# ------------------------------------------------------------------
+# Our implementation
+# ------------------------------------------------------------------
+
+
+class Step:
+    """One step's device buffers and launches through the C ABI (inputs resident in HBM)."""
+
+    def __init__(self, log_msm: int, log_ntt: int, seed: int) -> None:
+        import numpy as np
+        import torch
+
+        from zkgpu import _native, curve_gpu, workloads as wl
+        from zkgpu.field256_gpu import BN254_FR
+
+        self.torch, self.np, self.native, self.wl = torch, np, _native, wl
+        self.lib = _native.lib()
+        self.n, self.m = 1 << log_msm, 1 << log_ntt
+        n, m = self.n, self.m
+        self.k_host = wl.base_scalars(seed, n)
+        self.bases = curve_gpu.mul_generator(self.k_host)  # (n, 2, 4) Montgomery, resident
+        self.sc_uniform_host = wl.uniform_fr(seed + 1, n)
+        self.sc_skewed_host = wl.skewed_scalars(seed + 2, n)
+        self.sc_uniform = torch.from_numpy(self.sc_uniform_host).cuda()
+        self.sc_skewed = torch.from_numpy(self.sc_skewed_host).cuda()
+        self.ntt_plain_host = wl.uniform_fr(seed + 3, m)
+        self.ntt_in = BN254_FR.to_montgomery(self.ntt_plain_host)
+        self.ntt_out = torch.empty_like(self.ntt_in)
+        self.field = BN254_FR._field()
+        self.w = int(self.lib.zkb_msm_default_window(n))
+        self.msm_ws_bytes = int(self.lib.zkb_msm_workspace_bytes(n, self.w))
+        self.msm_ws = torch.empty(self.msm_ws_bytes, dtype=torch.uint8, device="cuda")
+        self.ntt_ws_bytes = int(self.lib.zkb_ntt_workspace_bytes(m))
+        self.ntt_ws = torch.empty(max(self.ntt_ws_bytes, 1), dtype=torch.uint8, device="cuda")
+        self.result = torch.empty((2, 9), dtype=torch.int64, device="cuda")
+        self.coset = _native.u64_array(_native.limbs(COSET))
+        torch.cuda.synchronize()
+
+    def msm(self, scalars, out_row: int) -> None:
+        s = self.native.stream_ptr()
+        self.native.check(self.lib.zkb_msm(
+            self.bases.data_ptr(), scalars.data_ptr(), self.n, self.w, self.result[out_row].data_ptr(),
+            self.msm_ws.data_ptr(), self.msm_ws_bytes, s))
+
+    def ntt(self, coset: bool) -> None:
+        s = self.native.stream_ptr()
+        self.native.check(self.lib.zkb_ntt(
+            self.field, self.ntt_in.data_ptr(), self.ntt_out.data_ptr(), self.m, 0, None,
+            self.coset if coset else None, self.ntt_ws.data_ptr(), self.ntt_ws_bytes, s))
+
+    def parts(self):
+        return (("msm_uniform", lambda: self.msm(self.sc_uniform, 0)),
+                ("msm_skewed", lambda: self.msm(self.sc_skewed, 1)),
+                ("ntt", lambda: self.ntt(False)),
+                ("coset_ntt", lambda: self.ntt(True)))
+
+
+def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
+    import numpy as np
+    import torch
+
+    from zkgpu import _native, msm_gpu
+    from zkgpu.field256_gpu import BN254_FR
+
+    torch.cuda.set_device(local_rank)
+    device = torch.device("cuda", local_rank)
+    dist = init_dist(world, "nccl")
+    log_msm, log_ntt = WORKLOADS[args.workload]
+    step = Step(log_msm, log_ntt, seed=10 + 100 * rank)
+
+    def one_step() -> None:
+        for _, fn in step.parts():
+            fn()
+
+    for _ in range(args.warmup):
+        one_step()
+    torch.cuda.synchronize()
+
+    # ---- timed region: device time per step, inputs resident in HBM
+    parts = step.parts()
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(len(parts) + 1)] for _ in range(args.steps)]
+    launches0 = int(_native.lib().zkb_launch_count())
+    barrier(dist, device)
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clocks:
+        start = torch.cuda.Event(enable_timing=True)
+        stop = torch.cuda.Event(enable_timing=True)
+        start.record()
+        for k in range(args.steps):
+            ev[k][0].record()
+            for j, (_, fn) in enumerate(parts):
+                fn()
+                ev[k][j + 1].record()
+        stop.record()
+        torch.cuda.synchronize()
+    barrier(dist, device)
+    launches = int(_native.lib().zkb_launch_count()) - launches0
+    elapsed = start.elapsed_time(stop)
+    ms_step = max_over_ranks(elapsed / args.steps, dist, device)
+    part_ms = {name: sum(ev[k][j].elapsed_time(ev[k][j + 1]) for k in range(args.steps)) / args.steps
+               for j, (name, _) in enumerate(parts)}
+
+    # ---- stage profile (library-recorded CUDA events on the launch stream), separate steps
+    _native.profile_enable(True)
+    for _ in range(max(2, min(args.steps, 5))):
+        step.msm(step.sc_uniform, 0)
+    prof_msm = _native.profile_report()
+    _native.profile_enable(False)
+    _native.profile_enable(True)
+    for _ in range(max(2, min(args.steps, 5))):
+        step.ntt(False)
+    prof_ntt = _native.profile_report()
+    _native.profile_enable(False)
+    torch.cuda.synchronize()
+
+    # ---- roofline of the dominant kernel: MSM bucket accumulation (integer-multiply bound)
+    clk = clocks.summary()
+    peaks = _peaks()
+    sm_count = torch.cuda.get_device_properties(device).multi_processor_count
+    mhz = clk.get("sm_mhz") or peaks.get("clocks_under_load", {}).get("sm_mhz_median") or peaks.get("sm_max_mhz", 1965.0)
+    imad_peak_t = sm_count * 64 * mhz * 1e6 / 1e12  # T IMAD/s at the sampled clock
+    madds = nonzero_digits(step.sc_uniform_host, step.w)
+    acc_count, acc_ms = prof_msm.get("msm_acc_points", (1, float("nan")))
+    acc_avg_ms = acc_ms / max(acc_count, 1)
+    imad = madds * MULMOD_PER_MADD * IMAD_PER_MULMOD
+    achieved = imad / (acc_avg_ms * 1e-3) / 1e12
+    acc_bytes = madds * (64 + 8) + 2 * (-(-madds // 64)) * 132  # point gathers + sorted pairs + partial slots
+    hbm_peak = peaks.get("hbm_gbs")
+    traffic = _profile_traffic("msm_acc_points", step.n)
+    roofline = {
+        "kernel": "k_msm_acc_points (bucket accumulation, uniform scalars)",
+        "bound": "imad",
+        "achieved": round(achieved, 3),
+        "peak": round(imad_peak_t, 3),
+        "unit": "TIMAD/s",
+        "frac": round(achieved / imad_peak_t, 4),
+        "traffic": traffic,
+        "peak_source": f"nominal issue rate: {sm_count} SMs x 64 IMAD/clk x {mhz:.0f} MHz (median SM clock sampled)",
+        "work_per_launch": f"{madds} mixed additions x {MULMOD_PER_MADD} mulmod x {IMAD_PER_MULMOD} IMAD",
+        "launch_ms": round(acc_avg_ms, 4),
+        "hbm": {"achieved": round(acc_bytes / (acc_avg_ms * 1e-3) / 1e9, 1), "peak": hbm_peak, "unit": "GB/s",
+                "frac": round(acc_bytes / (acc_avg_ms * 1e-3) / 1e9 / hbm_peak, 4) if hbm_peak else None,
+                "source": "measured (MEASURED_PEAKS.json)" if hbm_peak else None},
+    }
+    # NTT passes: bytes moved (read + write of 32-byte rows per pass) against HBM
+    ntt_pass_ms = sum(v[1] for k, v in prof_ntt.items() if k.startswith("ntt_")) / max(2, min(args.steps, 5))
+    n_passes = sum(v[0] for k, v in prof_ntt.items() if k.startswith("ntt_")) / max(2, min(args.steps, 5))
+    ntt_bytes = 64 * step.m * n_passes
+    ntt_gbs = ntt_bytes / (ntt_pass_ms * 1e-3) / 1e9
+    ntt_mulmods = (step.m // 2) * log_ntt + 2 * step.m * (n_passes - 1)
+    ntt_roof = {"bytes_per_launch": int(ntt_bytes), "ms": round(ntt_pass_ms, 4), "achieved_gbs": round(ntt_gbs, 1),
+                "hbm_frac": round(ntt_gbs / hbm_peak, 4) if hbm_peak else None,
+                "imad_frac": round(ntt_mulmods * IMAD_PER_MULMOD / (ntt_pass_ms * 1e-3) / 1e12 / imad_peak_t, 4),
+                "passes": n_passes}
+
+    # ---- end to end through the public API, pinned host buffers, copies inside the timed region
+    e2e = None
+    if not args.skip_e2e:
+        e2e = _run_e2e(args, step, dist, device, log_msm, log_ntt)
+
+    cpu = None
+    if rank == 0 and not args.skip_cpu_baseline:
+        cpu = cpu_baseline_sample(step, threads=1)
+
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank != 0:
+        return None
+    line = {
+        "metric": METRIC, "value": round(ms_step, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_step, 3), "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32 (8x32-bit limb Montgomery, exact)", "data": "synthetic (seeded)",
+        "config": {"workload": f"msm-2^{log_msm}-uniform+skewed, ntt-2^{log_ntt}+coset",
+                   "msm_points": step.n, "msm_window": step.w, "ntt_size": step.m, "coset": COSET,
+                   "scalars": ["uniform [0,r)", "skewed 60% {0,1} / 20% < 2^32 / 20% uniform"],
+                   "l2": "every input larger than the 126 MB L2 (bases 256 MiB, NTT 512 MiB)",
+                   "parallelism": f"replicas x{world}"},
+        "parts_ms": {k: round(v, 3) for k, v in part_ms.items()},
+        "stages_ms": {k: round(v[1] / v[0], 4) for k, v in {**prof_msm, **prof_ntt}.items()},
+        "roofline": roofline,
+        "ntt_roofline": ntt_roof,
+        "gpu_launches": launches,
+        "clocks": clk,
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+    }
+    return line
+
+
+def _profile_traffic(kernel: str, n: int) -> float | None:
+    """DRAM bytes per launch of *kernel* from a committed ncu summary (profiles/*.txt lines
+    `traffic <kernel> <points> <bytes>`), scaled to n points; None when not captured yet."""
+    for f in sorted((ROOT / "profiles").glob("*.txt")):
+        for line in f.read_text().splitlines():
+            parts = line.split()
+            if len(parts) == 4 and parts[0] == "traffic" and parts[1] == kernel:
+                try:
+                    return round(float(parts[3]) * n / float(parts[2]))
+                except ValueError:
+                    continue
+    return None
+
+
+def _run_e2e(args, step: Step, dist, device, log_msm: int, log_ntt: int) -> dict:
+    """The same step through the public API with pinned host inputs and host results."""
+    import numpy as np
+    import torch
+
+    from zkgpu import curve_gpu, msm_gpu
+    from zkgpu.field256_gpu import BN254_FQ, BN254_FR
+
+    # host inputs: plain affine coordinates, plain scalars, plain NTT input (pinned)
+    plain = BN254_FQ.from_montgomery(step.bases.reshape(-1, 4)).reshape(-1, 2, 4).cpu().pin_memory()
+    su = torch.from_numpy(step.sc_uniform_host).pin_memory()
+    ss = torch.from_numpy(step.sc_skewed_host).pin_memory()
+    xin = torch.from_numpy(step.ntt_plain_host).pin_memory()
+    yout = torch.empty_like(xin).pin_memory()
+    h2d = 2 * (plain.numel() * 8) + su.numel() * 8 + ss.numel() * 8 + 2 * xin.numel() * 8
+    d2h = 2 * yout.numel() * 8 + 2 * 80
+
+    def e2e_step() -> None:
+        msm_gpu.msm_pippenger_affine(plain, su, window_size=None)
+        msm_gpu.msm_pippenger_affine(plain, ss, window_size=None)
+        for coset in (None, COSET):
+            y = BN254_FR.from_montgomery(BN254_FR.ntt(BN254_FR.to_montgomery(xin), coset=coset))
+            yout.copy_(y)
+
+    steps = max(2, min(args.steps, 5))
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    torch.cuda.synchronize()
+    barrier(dist, device)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(steps):
+        e2e_step()
+    b.record()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(a.elapsed_time(b) / steps, dist, device)
+    return {"value": round(ms, 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+            "steps": steps, "api": "zkgpu.msm_gpu.msm_pippenger_affine x2, Field256.to_montgomery/ntt/from_montgomery x2"}
+
+
+# ------------------------------------------------------------------
+# CPU baseline: the oracle (C port of the reference's CPU algorithms)
+# ------------------------------------------------------------------
+
+
+def _timed(fn) -> float:
+    t0 = time.perf_counter()
+    fn()
+    return time.perf_counter() - t0
+
+
+def cpu_estimate(bases_h, sc_u, sc_s, ntt_h, log_ntt: int, threads: int, full: bool) -> tuple[float, str]:
+    """Estimated ms of one step of the reference's CPU algorithms (the C oracle).
+
+    MSM at the reference's window for n (w = 16 at 2^22, zkgpu/msm.py:112-121):
+    windows are timed individually at full n and summed as w0 + w1 + (W - 2) w2
+    (windows 2.. hold the same digit statistics; w0/w1 carry the small scalars).
+    NTT: the bit-reversal copy plus a sample of butterfly stages (each stage is
+    n/2 butterflies), scaled to all log2 n stages; coset adds its scaling pass.
+    With full=True every window and stage runs (no scaling).
+    """
+    from oracle import c_oracle as co
+    from oracle import pyoracle as po
+
+    n = bases_h.shape[0]
+    w = po.pippenger_window_size(n)
+    W = -(-SCALAR_BITS // w)
+    total = 0.0
+    notes = []
+    for name, sc in (("uniform", sc_u), ("skewed", sc_s)):
+        if full:
+            t = _timed(lambda sc=sc: co.msm(bases_h, sc, w, threads=threads))
+        else:
+            t0 = _timed(lambda sc=sc: co.msm_window_sums(bases_h, sc, w, 0, 1, threads=1))
+            t1 = _timed(lambda sc=sc: co.msm_window_sums(bases_h, sc, w, 1, 2, threads=1))
+            t2 = _timed(lambda sc=sc: co.msm_window_sums(bases_h, sc, w, 2, 3, threads=1))
+            t = t0 + t1 + (W - 2) * t2
+        total += t
+        notes.append(f"msm {name} 2^{n.bit_length() - 1} w={w}: {t * 1e3:.0f} ms")
+    m = ntt_h.shape[0]
+    if full:
+        t_ntt = _timed(lambda: co.ntt(ntt_h, threads=threads))
+        t_coset = _timed(lambda: co.ntt(ntt_h, coset=COSET, threads=threads))
+    else:
+        sample = 2
+        t_rev = _timed(lambda: co.ntt(ntt_h, threads=threads, stages=(0, 0)))
+        t_st = (_timed(lambda: co.ntt(ntt_h, threads=threads, stages=(0, sample))) - t_rev) / sample
+        t_scale = _timed(lambda: co.ntt(ntt_h, coset=COSET, threads=threads, stages=(0, 0))) - t_rev
+        t_ntt = t_rev + log_ntt * t_st
+        t_coset = t_ntt + max(t_scale, 0.0)
+    total += t_ntt + t_coset
+    notes.append(f"ntt 2^{log_ntt}: {t_ntt * 1e3:.0f} ms, coset: {t_coset * 1e3:.0f} ms")
+    return total * 1e3, "; ".join(notes)
+
+
+def cpu_baseline_sample(step: Step, threads: int) -> dict:
+    from oracle import c_oracle as co
+
+    bases_h = step.bases.cpu().numpy()
+    ntt_h = step.ntt_in.cpu().numpy()
+    log_ntt = step.m.bit_length() - 1
+    ms, notes = cpu_estimate(bases_h, step.sc_uniform_host, step.sc_skewed_host, ntt_h, log_ntt, threads, False)
+    return {"value": round(ms, 1), "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": "C port of the reference's CPU algorithms (oracle/zk_oracle.c) on the same inputs: "
+                      "MSM windows 0, 1, 2 at full n scaled to all windows; NTT bit reversal + 2 of "
+                      f"{log_ntt} stages scaled; " + notes,
+            "host_cpus": os.cpu_count()}
+
+
+# ------------------------------------------------------------------
+# Reference arm
+# ------------------------------------------------------------------
+
+
+def run_reference(args, rank: int, world: int) -> dict | None:
+    """The reference's CPU algorithms (C port) on the same workload, all host threads."""
+    if rank != 0:
+        return None
+    import numpy as np
+
+    from oracle import c_oracle as co
+    from zkgpu import workloads as wl
+
+    log_msm, log_ntt = WORKLOADS[args.workload]
+    n, m = 1 << log_msm, 1 << log_ntt
+    threads = os.cpu_count() or 1
+    k = wl.base_scalars(10, n)
+    bases_h = co.mul_generator(k, threads=threads)
+    sc_u, sc_s = wl.uniform_fr(11, n), wl.skewed_scalars(12, n)
+    ntt_h = co.to_mont(co.FR, wl.uniform_fr(13, m))
+    # full workload per step when the host has the cores for it, else the bounded sample
+    full = threads >= 32
+    times = []
+    notes = ""
+    for i in range(args.warmup + args.steps):
+        ms, notes = cpu_estimate(bases_h, sc_u, sc_s, ntt_h, log_ntt, threads, full)
+        if i >= args.warmup:
+            times.append(ms)
+    value = statistics.mean(times)
+    sample = ("full step" if full else "bounded sample (MSM windows 0-2 at full n, NTT 2 of "
+              f"{log_ntt} stages, scaled)") + f" with {threads} threads; " + notes
+    return {
+        "impl": "reference", "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(value, 1), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64 (4x64-bit limb Montgomery, exact)",
+        "data": "synthetic (seeded)",
+        "config": {"workload": f"msm-2^{log_msm}-uniform+skewed, ntt-2^{log_ntt}+coset", "msm_points": n,
+                   "ntt_size": m, "coset": COSET},
+        "cpu_baseline": {"value": round(value, 1), "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[1])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--workload", choices=tuple(WORKLOADS), default="large")
+    ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--skip-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3  # at least three untimed steps
+    rank, world, local_rank = dist_env()
+    if args.impl == "reference":
+        line = run_reference(args, rank, world)
+    else:
+        line = run_ours(args, rank, world, local_rank)
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,184 @@
+/*
+ * zkb200.h — C ABI of libzkb200.so, the B200 (sm_100a) BN254 prover hot path.
+ *
+ * Every buffer argument is a DEVICE pointer unless stated otherwise; `stream`
+ * is a cudaStream_t (NULL = the legacy default stream). Calls are
+ * stream-ordered and return as soon as the work is queued; a result is ready
+ * once the stream has reached it. Every call returns ZKB_OK or an error code
+ * and leaves a message for zkb_last_error() (thread-local).
+ *
+ * Data layout (the reference's, zkgpu/field256_gpu.py:12-20 and
+ * zkgpu/curve_gpu.py:15-26):
+ *   field element  4 x uint64, little-endian limbs, Montgomery form a*2^256 mod p,
+ *                  canonical (< p); 32 bytes per row.
+ *   Jacobian point (X, Y, Z), 3 field elements (96 bytes); Z = 0 is the identity,
+ *                  stored as (ONE, ONE, 0).
+ *   affine point   (x, y), 2 field elements (64 bytes); never the identity.
+ *
+ * Each entry point below names the reference interface it replaces. The
+ * reference has no native FFI: its GPU path launches CuPy RawKernels from
+ * Python, so these functions take the place of those launches together with
+ * the host-side argument handling around them.
+ */
+#ifndef ZKB200_H
+#define ZKB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+#define ZKB_OK 0
+#define ZKB_EINVAL 1      /* bad argument value (Python: ValueError) */
+#define ZKB_ETYPE 2       /* bad buffer shape or type (Python: TypeError) */
+#define ZKB_ECUDA 3       /* CUDA error (Python: RuntimeError) */
+#define ZKB_ENOTONCURVE 4 /* an input point is not on y^2 = x^3 + 3 (ValueError) */
+#define ZKB_EWORKSPACE 5  /* workspace too small (ValueError) */
+#define ZKB_ETIMEOUT 6    /* a bounded device wait gave up (RuntimeError) */
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* zkb_last_error(void);
+
+/* ABI version of this library (major * 100 + minor). */
+int zkb_version(void);
+
+/* ---- fields --------------------------------------------------------------- */
+
+/* A prime field's Montgomery parameters. Plain data: filled by zkb_field_init,
+ * copied by value, never freed. */
+typedef struct zkb_field {
+  uint64_t modulus[4]; /* p, odd, 3 <= p < 2^255 */
+  uint64_t one[4];     /* R mod p, R = 2^256 (Montgomery one) */
+  uint64_t r2[4];      /* R^2 mod p (converts into Montgomery form) */
+  uint64_t ninv;       /* -p^-1 mod 2^64 (the reference's ZK_NINV) */
+  int32_t kind;        /* ZKB_FIELD_GENERIC, ZKB_FIELD_BN254_FR or ZKB_FIELD_BN254_FQ */
+  int32_t reserved;
+} zkb_field;
+
+#define ZKB_FIELD_GENERIC 0
+#define ZKB_FIELD_BN254_FR 1
+#define ZKB_FIELD_BN254_FQ 2
+
+/* Replaces Field256.__init__ (zkgpu/field256_gpu.py:277-288): validates the
+ * modulus (odd, in [3, 2^255); ZKB_EINVAL otherwise) and computes R mod p,
+ * R^2 mod p and -p^-1 mod 2^64 on the host. Host pointers. */
+int zkb_field_init(zkb_field* f, const uint64_t modulus[4]);
+
+/* Replaces the zk256_mul / zk256_add / zk256_sub launches with their
+ * single-row broadcast (zkgpu/field256_gpu.py:172-191, :466-473):
+ * out[i] = a[i * a_step] OP b[i * b_step] for i < n, where a_step and b_step
+ * are 1, or 0 to broadcast one row. n = 0 is a no-op. out may alias a or b. */
+int zkb_field_mul(const zkb_field* f, const uint64_t* a, int64_t a_step, const uint64_t* b,
+                  int64_t b_step, uint64_t* out, int64_t n, void* stream);
+int zkb_field_add(const zkb_field* f, const uint64_t* a, int64_t a_step, const uint64_t* b,
+                  int64_t b_step, uint64_t* out, int64_t n, void* stream);
+int zkb_field_sub(const zkb_field* f, const uint64_t* a, int64_t a_step, const uint64_t* b,
+                  int64_t b_step, uint64_t* out, int64_t n, void* stream);
+
+/* Replaces Field256.from_ints' device step (zkgpu/field256_gpu.py:307-310):
+ * out[i] = Montgomery form of the plain value in[i]. For BN254 fields any
+ * 256-bit value is accepted and reduced mod p on the device; for other moduli
+ * in[i] must already be below p. */
+int zkb_field_to_mont(const zkb_field* f, const uint64_t* in, uint64_t* out, int64_t n,
+                      void* stream);
+
+/* Replaces Field256.to_ints' device step (zkgpu/field256_gpu.py:318-319):
+ * out[i] = the plain canonical value of Montgomery row in[i]. */
+int zkb_field_from_mont(const zkb_field* f, const uint64_t* in, uint64_t* out, int64_t n,
+                        void* stream);
+
+/* ---- NTT ------------------------------------------------------------------ */
+
+/* Device workspace (bytes) zkb_ntt needs for a transform of n rows. */
+size_t zkb_ntt_workspace_bytes(int64_t n);
+
+/* Replaces Field256.ntt / _ntt_on_gpu (zkgpu/field256_gpu.py:347-387) and the
+ * GPU coset form of Radix2Domain.coset_fft / coset_ifft (zkgpu/domain.py:122-135):
+ *   forward:  out[k] = sum_j in[j] * g^j * w^(j k)
+ *   inverse:  out[j] = n^-1 * g^-j * sum_k in[k] * w^(-j k)
+ * in natural order, with w a primitive n-th root of unity and g the coset
+ * offset (g = 1 when `coset` is NULL). n must be a power of two, 1 <= n <= 2^28.
+ * `omega` (host, plain canonical value of w) may be NULL for BN254 Fr, which
+ * then uses 5^((r-1)/n) (zkgpu/ntt.py:98-124). `coset` is a host pointer to g's
+ * plain value, or NULL. `in` is not modified; out must not alias in. */
+int zkb_ntt(const zkb_field* f, const uint64_t* in, uint64_t* out, int64_t n, int invert,
+            const uint64_t* omega, const uint64_t* coset, void* workspace,
+            size_t workspace_bytes, void* stream);
+
+/* ---- BN254 G1 ------------------------------------------------------------- */
+
+/* Replace the zk_g1_add / zk_g1_add_affine / zk_g1_double launches
+ * (zkgpu/curve_gpu.py:236-274, :394-414, :446-462): EFD add-2007-bl,
+ * madd-2007-bl and dbl-2009-l with the reference's special cases, so the
+ * Jacobian coordinates are exactly the reference's. a_step / b_step as for
+ * the field ops. out may alias the inputs. */
+int zkb_g1_add(const uint64_t* a, int64_t a_step, const uint64_t* b, int64_t b_step,
+               uint64_t* out, int64_t n, void* stream);
+int zkb_g1_add_affine(const uint64_t* a, int64_t a_step, const uint64_t* b, int64_t b_step,
+                      uint64_t* out, int64_t n, void* stream);
+int zkb_g1_double(const uint64_t* a, uint64_t* out, int64_t n, void* stream);
+
+/* Replaces the device half of curve_gpu.from_device and curve.from_jacobian
+ * (zkgpu/curve_gpu.py:384-386, zkgpu/curve.py:221-233): out is (n, 2, 4)
+ * plain canonical affine coordinates, with (0, 0) for the identity. */
+int zkb_g1_to_affine(const uint64_t* jac, uint64_t* out, int64_t n, void* stream);
+
+/* Fixed-base scalar multiplication k_i G for the generator G = (1, 2), the
+ * reference's Point.__mul__ (zkgpu/curve.py:153-159) used to build base sets:
+ * k is (n, 4) plain 256-bit scalars (not 0 mod r), out is (n, 2, 4) affine
+ * rows in Montgomery form. */
+int zkb_g1_mul_generator(const uint64_t* k, uint64_t* out, int64_t n, void* stream);
+
+/* Replaces the on-curve validation that Point() performs for every MSM input
+ * (zkgpu/msm_gpu.py:441-442, zkgpu/curve.py:69-79), on the device:
+ * points is (n, 2, 4) affine in Montgomery form; *first_bad (a device int64)
+ * receives the smallest index whose point is off the curve, or -1. */
+int zkb_g1_check_affine(const uint64_t* points, int64_t n, int64_t* first_bad, void* stream);
+
+/* ---- MSM ------------------------------------------------------------------ */
+
+/* The library's default window size for n points. */
+int zkb_msm_default_window(int64_t n);
+
+/* Device workspace (bytes) zkb_msm needs for n points at window size w
+ * (w = 0: the default). */
+size_t zkb_msm_workspace_bytes(int64_t n, int window_size);
+
+/* Replaces msm_pippenger_gpu's device path (zkgpu/msm_gpu.py:336-377, :447-449)
+ * including the final window combination and affine conversion, which the
+ * reference runs on the CPU (zkgpu/msm.py:156-169, zkgpu/curve.py:221-233).
+ *   points   (n, 2, 4) affine BN254 G1 points in Montgomery form (valid points;
+ *            see zkb_g1_check_affine)
+ *   scalars  (n, 4) plain little-endian 256-bit integers; reduced mod r on the
+ *            device (the reference reduces mod r on the host)
+ *   result   device buffer of 9 uint64: x (4 limbs), y (4 limbs), both plain
+ *            canonical, then 1 if the sum is the point at infinity (x = y = 0)
+ *            else 0.
+ * window_size is in 1..20, or 0 for zkb_msm_default_window(n). Digits are
+ * signed, so a window of w bits has 2^(w-1) buckets. n = 0 gives infinity. */
+int zkb_msm(const uint64_t* points, const uint64_t* scalars, int64_t n, int window_size,
+            uint64_t* result, void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---- measurement -------------------------------------------------------- */
+
+/* Number of this library's own kernels launched so far in this process
+ * (sorting kernels of the CUB library are not counted). */
+uint64_t zkb_launch_count(void);
+
+/* Per-stage timing with CUDA events on the launching stream. on = 1 clears
+ * the record and starts recording the MSM and NTT stages; 0 stops. */
+void zkb_profile_enable(int on);
+
+/* Waits for the recorded events and writes one line per stage,
+ * "name count total_ms", into buf (host, len bytes, NUL-terminated).
+ * Returns the length the full report needs, including the NUL. */
+int zkb_profile_report(char* buf, size_t len);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ZKB200_H */

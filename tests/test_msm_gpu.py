@@ -1,0 +1,174 @@
+"""
+zkgpu.msm_gpu on the GPU: the affine result bit-exact against the
+reference's Pippenger on the same inputs (golden fixtures: its test cases and
+seeded 2^12 / 2^14 / 2^16 instances), every window size, skewed scalars, and
+at the config sizes (2^22 points) through size-independent identities and a
+2^16 subset against the C oracle.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+from conftest import golden, hs
+from oracle import c_oracle as co
+from oracle import pyoracle as po
+from zkgpu import _native, curve_gpu, msm_gpu
+from zkgpu import workloads as wl
+from zkgpu.curve import G, P, Point, R
+from zkgpu.msm_gpu import msm_pippenger_gpu, msm_pippenger_rows
+
+pytestmark = pytest.mark.gpu
+
+
+def expected_point(case) -> Point:
+    return Point.identity() if case["expected"] is None else Point(*hs(case["expected"]))
+
+
+def run_case(case, window_size=None) -> Point:
+    pts = [hs(p) for p in case["points"]]
+    sc = [int(s) for s in case["raw_scalars"]] if "raw_scalars" in case else hs(case["scalars"])
+    return msm_pippenger_gpu(
+        np.array([p[0] for p in pts], dtype=object),
+        np.array([p[1] for p in pts], dtype=object),
+        np.array(sc, dtype=object),
+        window_size=window_size,
+    )
+
+
+@pytest.mark.parametrize("window_size", [None, 1, 2, 3, 5, 8, 11, 13, 16])
+@pytest.mark.parametrize("case", golden("msm.json")["cases"], ids=lambda c: c["name"])
+def test_msm_matches_the_references(case, window_size):
+    assert run_case(case, window_size) == expected_point(case)
+
+
+def _bases(n: int, seed: int):
+    return curve_gpu.mul_generator(wl.base_scalars(seed, n))
+
+
+@pytest.mark.parametrize("case", golden("msm.json")["seeded"], ids=lambda c: f"{c['kind']}-{c['n']}")
+def test_seeded_msm_matches_the_references(case):
+    n = case["n"]
+    bases = _bases(n, case["base_seed"])
+    gen = wl.uniform_fr if case["kind"] == "uniform" else wl.skewed_scalars
+    sc = gen(case["scalar_seed"], n)
+    for w in (None, 4, 9, 12, 16):
+        assert msm_pippenger_rows(bases, sc, window_size=w) == expected_point(case), w
+
+
+def _msm_raw(points, scalars, n, w):
+    """zkb_msm through the C ABI directly, for window sizes above the API's 16."""
+    import torch
+
+    lib = _native.lib()
+    ws_bytes = lib.zkb_msm_workspace_bytes(n, w)
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device="cuda")
+    out = torch.empty(9, dtype=torch.int64, device="cuda")
+    _native.check(lib.zkb_msm(points.data_ptr(), scalars.data_ptr(), n, w, out.data_ptr(), ws.data_ptr(),
+                              ws_bytes, _native.stream_ptr()))
+    return msm_gpu._result_point(out.cpu().numpy().view(np.uint64))
+
+
+@pytest.mark.parametrize("w", [17, 18, 20])
+def test_internal_windows_beyond_16(w):
+    case = golden("msm.json")["seeded"][0]
+    n = case["n"]
+    import torch
+
+    bases = _bases(n, case["base_seed"])
+    gen = wl.uniform_fr if case["kind"] == "uniform" else wl.skewed_scalars
+    sc = torch.from_numpy(gen(case["scalar_seed"], n)).cuda()
+    assert _msm_raw(bases, sc, n, w) == expected_point(case)
+
+
+def test_bucket_edge_cases():
+    assert msm_pippenger_gpu([G.x, G.x], [G.y, P - G.y], [7, 7]) == Point.identity()
+    assert msm_pippenger_gpu([G.x, G.x], [G.y, G.y], [5, 5]) == Point(*po.scalar_mul(po.G, 10))
+    assert msm_pippenger_gpu([G.x, G.x], [G.y, G.y], [0, 0]) == Point.identity()
+
+
+def test_reduces_scalars_mod_r():
+    three = po.scalar_mul(po.G, 3)
+    for scalar in (-5, R, R + 7, 2**300 + 1):
+        assert msm_pippenger_gpu([three[0]], [three[1]], [scalar]) == Point(*po.scalar_mul(three, scalar % R))
+
+
+def test_returns_a_point():
+    assert msm_pippenger_gpu([], [], []) == Point.identity()
+    result = msm_pippenger_gpu([G.x], [G.y], [R])
+    assert isinstance(result, Point) and result.is_identity()
+    assert msm_pippenger_gpu([G.x, G.x], [G.y, G.y], [2, 3]) == Point(*po.scalar_mul(po.G, 5))
+
+
+def test_off_curve_points_are_rejected_on_the_device():
+    with pytest.raises(ValueError, match=r"\(1, 3\) is not on the BN254 curve"):
+        msm_pippenger_gpu([1], [3], [5])
+    with pytest.raises(ValueError, match="not on the BN254 curve"):
+        msm_pippenger_gpu([G.x, 1, G.x], [G.y, 3, G.y], [1, 2, 3])
+
+
+def test_heavy_bucket_and_boolean_scalars():
+    pts = [po.scalar_mul(po.G, k) for k in range(1, 301)]
+    xs, ys = [p[0] for p in pts], [p[1] for p in pts]
+    scalar = 2**200 + 12345
+    assert msm_pippenger_gpu(xs, ys, [scalar] * 300) == Point(*po.scalar_mul(po.G, sum(range(1, 301)) * scalar % R))
+    bools = [k % 3 != 0 for k in range(300)]
+    want = po.msm_double_and_add(pts, [int(b) for b in bools])
+    assert msm_pippenger_gpu(xs, ys, [int(b) for b in bools], window_size=9) == Point(*want)
+
+
+def test_self_test_passes():
+    msm_gpu.compile_kernels()
+
+
+# ------------------------------------------------------------------
+# Config sizes: 2^22 points (config 3), uniform and skewed scalars
+# ------------------------------------------------------------------
+
+
+@pytest.fixture(scope="module")
+def big_bases():
+    return _bases(1 << 22, 3)
+
+
+def test_2_22_subset_matches_c_oracle(big_bases):
+    """Config 3's subset check: the first 2^16 of the 2^22 inputs against the C oracle."""
+    m = 1 << 16
+    for sc in (wl.uniform_fr(3, 1 << 22)[:m], wl.skewed_scalars(4, 1 << 22)[:m]):
+        got = msm_pippenger_rows(big_bases[:m], sc)
+        out = co.msm(big_bases[:m].cpu().numpy(), sc, 16, threads=os.cpu_count() or 1)
+        want = Point.identity() if out[8] else Point(*wl.rows_to_ints(out[:8].reshape(2, 4)))
+        assert got == want
+
+
+@pytest.mark.parametrize("kind", ["uniform", "skewed"])
+def test_2_22_linearity_and_split(big_bases, kind):
+    """sum s_i P_i + sum t_i P_i == sum (s_i + t_i) P_i, and the sum of two halves is the whole."""
+    n = 1 << 22
+    gen = wl.uniform_fr if kind == "uniform" else wl.skewed_scalars
+    s, t = gen(3, n), gen(4, n)
+    whole_s = msm_pippenger_rows(big_bases, s)
+    whole_t = msm_pippenger_rows(big_bases, t)
+    st = np.array(wl.rows_to_ints(s), dtype=object) + np.array(wl.rows_to_ints(t), dtype=object)
+    st_rows = np.array([[(v % R >> (64 * j)) & (2**64 - 1) for j in range(4)] for v in st], dtype=np.uint64)
+    assert whole_s + whole_t == msm_pippenger_rows(big_bases, st_rows)
+    h = n // 2 + 12345
+    assert msm_pippenger_rows(big_bases[:h], s[:h]) + msm_pippenger_rows(big_bases[h:], s[h:]) == whole_s
+    assert not whole_s.is_identity()
+
+
+def test_workspace_too_small_is_an_error():
+    import torch
+
+    lib = _native.lib()
+    bases = _bases(64, 9)
+    sc = torch.from_numpy(wl.uniform_fr(9, 64)).cuda()
+    out = torch.empty(9, dtype=torch.int64, device="cuda")
+    status = lib.zkb_msm(bases.data_ptr(), sc.data_ptr(), 64, 8, out.data_ptr(), None, 0, _native.stream_ptr())
+    assert status == _native.ZKB_EWORKSPACE
+    assert "workspace" in _native.last_error()
+    assert ctypes.c_int(status).value == 5

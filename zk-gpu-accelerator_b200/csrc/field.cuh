@@ -1,0 +1,411 @@
+// field.cuh — 256-bit Montgomery arithmetic for sm_100a, 8 x 32-bit limbs.
+//
+// An element is the Montgomery form a*R mod p with R = 2^256, held as eight
+// little-endian 32-bit limbs. In memory one element is 32 bytes, so its bytes
+// are identical to the reference's (n, 4) uint64 rows (zkgpu/field256_gpu.py:12-20):
+// a row written by this code reads back as the same four 64-bit limbs.
+//
+// Contract (zkgpu/field256_gpu.py:22-30): the modulus is odd and below 2^255,
+// inputs are canonical (< p), and every function returns canonical output, so
+// results are bit-identical to any other correct Montgomery implementation with
+// R = 2^256 (the canonical representative of a*b*R^-1 mod p is unique).
+//
+// Multiplication is CIOS (Koc, Acar, Kaliski 1996) over 32-bit words. Each of
+// the eight outer steps adds a*b[i], then m*p with m = t[0] * (-p^-1 mod 2^32),
+// and drops the zero low word. Between steps t < 2p; during a step the running
+// total is below 2^32 * 2p < 2^288, so nine words of state suffice and the top
+// word never carries out. Each row is two carry chains written as inline PTX
+// (mad.lo.cc / madc.lo.cc for the low halves of the partial products, then
+// mad.hi.cc / madc.hi.cc for the high halves one word up), so the compiler
+// never has to materialise a 64-bit product or a carry in a general register.
+#pragma once
+#include <cstdint>
+
+namespace zkb {
+
+// ---------------------------------------------------------------------------
+// Field policies: p(i), one(i) (= R mod p), r2(i) (= R^2 mod p), ninv
+// (= -p^-1 mod 2^32). Compile-time policies fold into immediates.
+// ---------------------------------------------------------------------------
+
+// BN254 scalar field r (zkgpu/field.py:17 FIELD_MODULUS).
+struct FrP {
+  __host__ __device__ __forceinline__ static constexpr uint32_t p(int i) {
+    constexpr uint32_t v[8] = {0xf0000001u, 0x43e1f593u, 0x79b97091u, 0x2833e848u,
+                               0x8181585du, 0xb85045b6u, 0xe131a029u, 0x30644e72u};
+    return v[i];
+  }
+  __host__ __device__ __forceinline__ static constexpr uint32_t one(int i) {
+    constexpr uint32_t v[8] = {0x4ffffffbu, 0xac96341cu, 0x9f60cd29u, 0x36fc7695u,
+                               0x7879462eu, 0x666ea36fu, 0x9a07df2fu, 0x0e0a77c1u};
+    return v[i];
+  }
+  __host__ __device__ __forceinline__ static constexpr uint32_t r2(int i) {
+    constexpr uint32_t v[8] = {0xae216da7u, 0x1bb8e645u, 0xe35c59e3u, 0x53fe3ab1u,
+                               0x53bb8085u, 0x8c49833du, 0x7f4e44a5u, 0x0216d0b1u};
+    return v[i];
+  }
+  __host__ __device__ __forceinline__ static constexpr uint32_t ninv() { return 0xefffffffu; }
+};
+
+// BN254 base field p (zkgpu/curve.py:29 P): curve coordinates.
+struct FqP {
+  __host__ __device__ __forceinline__ static constexpr uint32_t p(int i) {
+    constexpr uint32_t v[8] = {0xd87cfd47u, 0x3c208c16u, 0x6871ca8du, 0x97816a91u,
+                               0x8181585du, 0xb85045b6u, 0xe131a029u, 0x30644e72u};
+    return v[i];
+  }
+  __host__ __device__ __forceinline__ static constexpr uint32_t one(int i) {
+    constexpr uint32_t v[8] = {0xc58f0d9du, 0xd35d438du, 0xf5c70b3du, 0x0a78eb28u,
+                               0x7879462cu, 0x666ea36fu, 0x9a07df2fu, 0x0e0a77c1u};
+    return v[i];
+  }
+  __host__ __device__ __forceinline__ static constexpr uint32_t r2(int i) {
+    constexpr uint32_t v[8] = {0x538afa89u, 0xf32cfc5bu, 0xd44501fbu, 0xb5e71911u,
+                               0x0a417ff6u, 0x47ab1effu, 0xcab8351fu, 0x06d89f71u};
+    return v[i];
+  }
+  __host__ __device__ __forceinline__ static constexpr uint32_t ninv() { return 0xe4866389u; }
+};
+
+// Any odd modulus in [3, 2^255), passed by value in kernel parameters
+// (Field256(modulus) for moduli other than BN254's, zkgpu/field256_gpu.py:277-288).
+struct FieldRT {
+  uint32_t P[8];
+  uint32_t ONE[8];
+  uint32_t R2[8];
+  uint32_t NINV;
+  __host__ __device__ __forceinline__ uint32_t p(int i) const { return P[i]; }
+  __host__ __device__ __forceinline__ uint32_t one(int i) const { return ONE[i]; }
+  __host__ __device__ __forceinline__ uint32_t r2(int i) const { return R2[i]; }
+  __host__ __device__ __forceinline__ uint32_t ninv() const { return NINV; }
+};
+
+// ---------------------------------------------------------------------------
+// Loads and stores: one element is two 16-byte vectors.
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ void fe_load(uint32_t r[8], const void* src) {
+  const uint4* s = reinterpret_cast<const uint4*>(src);
+  uint4 lo = s[0], hi = s[1];
+  r[0] = lo.x; r[1] = lo.y; r[2] = lo.z; r[3] = lo.w;
+  r[4] = hi.x; r[5] = hi.y; r[6] = hi.z; r[7] = hi.w;
+}
+
+// Read-only, streamed once: bypass L1 allocation.
+__device__ __forceinline__ void fe_load_nc(uint32_t r[8], const void* src) {
+  const uint4* s = reinterpret_cast<const uint4*>(src);
+  uint4 lo = __ldg(s), hi = __ldg(s + 1);
+  r[0] = lo.x; r[1] = lo.y; r[2] = lo.z; r[3] = lo.w;
+  r[4] = hi.x; r[5] = hi.y; r[6] = hi.z; r[7] = hi.w;
+}
+
+__device__ __forceinline__ void fe_store(void* dst, const uint32_t a[8]) {
+  uint4* d = reinterpret_cast<uint4*>(dst);
+  d[0] = make_uint4(a[0], a[1], a[2], a[3]);
+  d[1] = make_uint4(a[4], a[5], a[6], a[7]);
+}
+
+__device__ __forceinline__ void fe_copy(uint32_t r[8], const uint32_t a[8]) {
+#pragma unroll
+  for (int j = 0; j < 8; ++j) r[j] = a[j];
+}
+
+__device__ __forceinline__ void fe_zero(uint32_t r[8]) {
+#pragma unroll
+  for (int j = 0; j < 8; ++j) r[j] = 0;
+}
+
+template <class F>
+__device__ __forceinline__ void fe_one(uint32_t r[8], const F& f) {
+#pragma unroll
+  for (int j = 0; j < 8; ++j) r[j] = f.one(j);
+}
+
+// Rows are canonical, so zero is all-zero limbs (zkgpu/curve_gpu.py:67-69).
+__device__ __forceinline__ bool fe_is_zero(const uint32_t a[8]) {
+  return (a[0] | a[1] | a[2] | a[3] | a[4] | a[5] | a[6] | a[7]) == 0;
+}
+
+__device__ __forceinline__ bool fe_eq(const uint32_t a[8], const uint32_t b[8]) {
+  uint32_t d = 0;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) d |= a[j] ^ b[j];
+  return d == 0;
+}
+
+// ---------------------------------------------------------------------------
+// t := t - p if t >= p, for t < 2p (branch-free; zkgpu/field256_gpu.py:76-94).
+// ---------------------------------------------------------------------------
+template <class F>
+__device__ __forceinline__ void fe_reduce_once(uint32_t t[8], const F& f) {
+  uint32_t d0, d1, d2, d3, d4, d5, d6, d7, bw;
+  asm("sub.cc.u32 %0, %9, %17;\n\t"
+      "subc.cc.u32 %1, %10, %18;\n\t"
+      "subc.cc.u32 %2, %11, %19;\n\t"
+      "subc.cc.u32 %3, %12, %20;\n\t"
+      "subc.cc.u32 %4, %13, %21;\n\t"
+      "subc.cc.u32 %5, %14, %22;\n\t"
+      "subc.cc.u32 %6, %15, %23;\n\t"
+      "subc.cc.u32 %7, %16, %24;\n\t"
+      "subc.u32 %8, 0, 0;"
+      : "=r"(d0), "=r"(d1), "=r"(d2), "=r"(d3), "=r"(d4), "=r"(d5), "=r"(d6), "=r"(d7), "=r"(bw)
+      : "r"(t[0]), "r"(t[1]), "r"(t[2]), "r"(t[3]), "r"(t[4]), "r"(t[5]), "r"(t[6]), "r"(t[7]),
+        "r"(f.p(0)), "r"(f.p(1)), "r"(f.p(2)), "r"(f.p(3)), "r"(f.p(4)), "r"(f.p(5)), "r"(f.p(6)),
+        "r"(f.p(7)));
+  // bw is all ones when t < p (the subtraction borrowed): keep t then.
+  t[0] = bw ? t[0] : d0;
+  t[1] = bw ? t[1] : d1;
+  t[2] = bw ? t[2] : d2;
+  t[3] = bw ? t[3] : d3;
+  t[4] = bw ? t[4] : d4;
+  t[5] = bw ? t[5] : d5;
+  t[6] = bw ? t[6] : d6;
+  t[7] = bw ? t[7] : d7;
+}
+
+// r = a + b mod p. a, b < p < 2^255, so a + b < 2^256 never carries out.
+// r may alias a or b (every input limb is read before any output is written).
+template <class F>
+__device__ __forceinline__ void fe_add(uint32_t r[8], const uint32_t a[8], const uint32_t b[8],
+                                       const F& f) {
+  uint32_t s[8];
+  asm("add.cc.u32 %0, %8, %16;\n\t"
+      "addc.cc.u32 %1, %9, %17;\n\t"
+      "addc.cc.u32 %2, %10, %18;\n\t"
+      "addc.cc.u32 %3, %11, %19;\n\t"
+      "addc.cc.u32 %4, %12, %20;\n\t"
+      "addc.cc.u32 %5, %13, %21;\n\t"
+      "addc.cc.u32 %6, %14, %22;\n\t"
+      "addc.u32 %7, %15, %23;"
+      : "=r"(s[0]), "=r"(s[1]), "=r"(s[2]), "=r"(s[3]), "=r"(s[4]), "=r"(s[5]), "=r"(s[6]), "=r"(s[7])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]),
+        "r"(b[0]), "r"(b[1]), "r"(b[2]), "r"(b[3]), "r"(b[4]), "r"(b[5]), "r"(b[6]), "r"(b[7]));
+  fe_reduce_once(s, f);
+  fe_copy(r, s);
+}
+
+// r = a - b mod p: subtract, then add p back under the borrow mask
+// (zkgpu/field256_gpu.py:148-169). r may alias a or b.
+template <class F>
+__device__ __forceinline__ void fe_sub(uint32_t r[8], const uint32_t a[8], const uint32_t b[8],
+                                       const F& f) {
+  uint32_t s[8], bw;
+  asm("sub.cc.u32 %0, %9, %17;\n\t"
+      "subc.cc.u32 %1, %10, %18;\n\t"
+      "subc.cc.u32 %2, %11, %19;\n\t"
+      "subc.cc.u32 %3, %12, %20;\n\t"
+      "subc.cc.u32 %4, %13, %21;\n\t"
+      "subc.cc.u32 %5, %14, %22;\n\t"
+      "subc.cc.u32 %6, %15, %23;\n\t"
+      "subc.cc.u32 %7, %16, %24;\n\t"
+      "subc.u32 %8, 0, 0;"
+      : "=r"(s[0]), "=r"(s[1]), "=r"(s[2]), "=r"(s[3]), "=r"(s[4]), "=r"(s[5]), "=r"(s[6]), "=r"(s[7]),
+        "=r"(bw)
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]),
+        "r"(b[0]), "r"(b[1]), "r"(b[2]), "r"(b[3]), "r"(b[4]), "r"(b[5]), "r"(b[6]), "r"(b[7]));
+  asm("add.cc.u32 %0, %0, %8;\n\t"
+      "addc.cc.u32 %1, %1, %9;\n\t"
+      "addc.cc.u32 %2, %2, %10;\n\t"
+      "addc.cc.u32 %3, %3, %11;\n\t"
+      "addc.cc.u32 %4, %4, %12;\n\t"
+      "addc.cc.u32 %5, %5, %13;\n\t"
+      "addc.cc.u32 %6, %6, %14;\n\t"
+      "addc.u32 %7, %7, %15;"
+      : "+r"(s[0]), "+r"(s[1]), "+r"(s[2]), "+r"(s[3]), "+r"(s[4]), "+r"(s[5]), "+r"(s[6]), "+r"(s[7])
+      : "r"(f.p(0) & bw), "r"(f.p(1) & bw), "r"(f.p(2) & bw), "r"(f.p(3) & bw), "r"(f.p(4) & bw),
+        "r"(f.p(5) & bw), "r"(f.p(6) & bw), "r"(f.p(7) & bw));
+  fe_copy(r, s);
+}
+
+// r = -a mod p (0 stays 0).
+template <class F>
+__device__ __forceinline__ void fe_neg(uint32_t r[8], const uint32_t a[8], const F& f) {
+  uint32_t z[8];
+  fe_zero(z);
+  fe_sub(r, z, a, f);
+}
+
+// ---------------------------------------------------------------------------
+// CIOS rows. t holds nine words t[0..8]; t[8] is zero on entry to a step.
+// ---------------------------------------------------------------------------
+
+// t += a * b (eight low halves into t[0..7] with the carry into t[8], then the
+// eight high halves into t[1..8]).
+__device__ __forceinline__ void cios_mul_row(uint32_t t[9], const uint32_t a[8], uint32_t b) {
+  asm("mad.lo.cc.u32 %0, %9, %17, %0;\n\t"
+      "madc.lo.cc.u32 %1, %10, %17, %1;\n\t"
+      "madc.lo.cc.u32 %2, %11, %17, %2;\n\t"
+      "madc.lo.cc.u32 %3, %12, %17, %3;\n\t"
+      "madc.lo.cc.u32 %4, %13, %17, %4;\n\t"
+      "madc.lo.cc.u32 %5, %14, %17, %5;\n\t"
+      "madc.lo.cc.u32 %6, %15, %17, %6;\n\t"
+      "madc.lo.cc.u32 %7, %16, %17, %7;\n\t"
+      "addc.u32 %8, %8, 0;\n\t"
+      "mad.hi.cc.u32 %1, %9, %17, %1;\n\t"
+      "madc.hi.cc.u32 %2, %10, %17, %2;\n\t"
+      "madc.hi.cc.u32 %3, %11, %17, %3;\n\t"
+      "madc.hi.cc.u32 %4, %12, %17, %4;\n\t"
+      "madc.hi.cc.u32 %5, %13, %17, %5;\n\t"
+      "madc.hi.cc.u32 %6, %14, %17, %6;\n\t"
+      "madc.hi.cc.u32 %7, %15, %17, %7;\n\t"
+      "madc.hi.u32 %8, %16, %17, %8;"
+      : "+r"(t[0]), "+r"(t[1]), "+r"(t[2]), "+r"(t[3]), "+r"(t[4]), "+r"(t[5]), "+r"(t[6]),
+        "+r"(t[7]), "+r"(t[8])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]),
+        "r"(b));
+}
+
+// t = (t + m * p) / 2^32 with m = t[0] * ninv, so the low word cancels.
+template <class F>
+__device__ __forceinline__ void cios_reduce_row(uint32_t t[9], const F& f) {
+  uint32_t m = t[0] * f.ninv();
+  asm("mad.lo.cc.u32 %0, %10, %9, %0;\n\t"
+      "madc.lo.cc.u32 %1, %11, %9, %1;\n\t"
+      "madc.lo.cc.u32 %2, %12, %9, %2;\n\t"
+      "madc.lo.cc.u32 %3, %13, %9, %3;\n\t"
+      "madc.lo.cc.u32 %4, %14, %9, %4;\n\t"
+      "madc.lo.cc.u32 %5, %15, %9, %5;\n\t"
+      "madc.lo.cc.u32 %6, %16, %9, %6;\n\t"
+      "madc.lo.cc.u32 %7, %17, %9, %7;\n\t"
+      "addc.u32 %8, %8, 0;\n\t"
+      "mad.hi.cc.u32 %1, %10, %9, %1;\n\t"
+      "madc.hi.cc.u32 %2, %11, %9, %2;\n\t"
+      "madc.hi.cc.u32 %3, %12, %9, %3;\n\t"
+      "madc.hi.cc.u32 %4, %13, %9, %4;\n\t"
+      "madc.hi.cc.u32 %5, %14, %9, %5;\n\t"
+      "madc.hi.cc.u32 %6, %15, %9, %6;\n\t"
+      "madc.hi.cc.u32 %7, %16, %9, %7;\n\t"
+      "madc.hi.u32 %8, %17, %9, %8;"
+      : "+r"(t[0]), "+r"(t[1]), "+r"(t[2]), "+r"(t[3]), "+r"(t[4]), "+r"(t[5]), "+r"(t[6]),
+        "+r"(t[7]), "+r"(t[8])
+      : "r"(m), "r"(f.p(0)), "r"(f.p(1)), "r"(f.p(2)), "r"(f.p(3)), "r"(f.p(4)), "r"(f.p(5)),
+        "r"(f.p(6)), "r"(f.p(7)));
+  // t[0] is now zero: drop it.
+#pragma unroll
+  for (int j = 0; j < 8; ++j) t[j] = t[j + 1];
+  t[8] = 0;
+}
+
+// r = a * b * 2^-256 mod p, canonical. r may alias a and/or b.
+template <class F>
+__device__ __forceinline__ void fe_mul(uint32_t r[8], const uint32_t a[8], const uint32_t b[8],
+                                       const F& f) {
+  uint32_t x[8], y[8], t[9];
+  fe_copy(x, a);
+  fe_copy(y, b);
+#pragma unroll
+  for (int j = 0; j < 9; ++j) t[j] = 0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    cios_mul_row(t, x, y[i]);
+    cios_reduce_row(t, f);
+  }
+  fe_reduce_once(t, f);
+  fe_copy(r, t);
+}
+
+template <class F>
+__device__ __forceinline__ void fe_sqr(uint32_t r[8], const uint32_t a[8], const F& f) {
+  fe_mul(r, a, a, f);
+}
+
+// r = 2a, 3a, 4a, 8a mod p.
+template <class F>
+__device__ __forceinline__ void fe_dbl(uint32_t r[8], const uint32_t a[8], const F& f) {
+  fe_add(r, a, a, f);
+}
+
+// Montgomery form of a plain canonical value: a * R^2 * R^-1 = aR
+// (zkgpu/field256_gpu.py:307-310).
+template <class F>
+__device__ __forceinline__ void fe_to_mont(uint32_t r[8], const uint32_t a[8], const F& f) {
+  uint32_t r2[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) r2[j] = f.r2(j);
+  fe_mul(r, a, r2, f);
+}
+
+// Plain value of a Montgomery-form element: aR * 1 * R^-1 = a
+// (zkgpu/field256_gpu.py:318-319).
+template <class F>
+__device__ __forceinline__ void fe_from_mont(uint32_t r[8], const uint32_t a[8], const F& f) {
+  uint32_t one[8] = {1, 0, 0, 0, 0, 0, 0, 0};
+  fe_mul(r, a, one, f);
+}
+
+// r = a^e for a 256-bit exponent e (little-endian limbs), left to right.
+template <class F>
+__device__ __noinline__ void fe_pow(uint32_t r[8], const uint32_t a[8], const uint32_t e[8],
+                                    const F& f) {
+  uint32_t acc[8], base[8];
+  fe_one(acc, f);
+  fe_copy(base, a);
+  for (int w = 7; w >= 0; --w) {
+    for (int bit = 31; bit >= 0; --bit) {
+      fe_sqr(acc, acc, f);
+      if ((e[w] >> bit) & 1u) fe_mul(acc, acc, base, f);
+    }
+  }
+  fe_copy(r, acc);
+}
+
+// r = a^-1 = a^(p-2) (Fermat); a must be non-zero.
+template <class F>
+__device__ __forceinline__ void fe_inv(uint32_t r[8], const uint32_t a[8], const F& f) {
+  uint32_t e[8];
+  // p - 2: p is odd, so only the low limb changes (p >= 3, no borrow).
+#pragma unroll
+  for (int j = 0; j < 8; ++j) e[j] = f.p(j);
+  e[0] -= 2u;
+  fe_pow(r, a, e, f);
+}
+
+// Compare a plain 256-bit value with p: true when a < p.
+template <class F>
+__device__ __forceinline__ bool fe_lt_p(const uint32_t a[8], const F& f) {
+  uint32_t d, bw;
+  asm("sub.cc.u32 %0, %2, %10;\n\t"
+      "subc.cc.u32 %0, %3, %11;\n\t"
+      "subc.cc.u32 %0, %4, %12;\n\t"
+      "subc.cc.u32 %0, %5, %13;\n\t"
+      "subc.cc.u32 %0, %6, %14;\n\t"
+      "subc.cc.u32 %0, %7, %15;\n\t"
+      "subc.cc.u32 %0, %8, %16;\n\t"
+      "subc.cc.u32 %0, %9, %17;\n\t"
+      "subc.u32 %1, 0, 0;"
+      : "=r"(d), "=r"(bw)
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]),
+        "r"(f.p(0)), "r"(f.p(1)), "r"(f.p(2)), "r"(f.p(3)), "r"(f.p(4)), "r"(f.p(5)), "r"(f.p(6)),
+        "r"(f.p(7)));
+  return bw != 0;
+}
+
+// a := a - p (no check; the caller knows a >= p).
+template <class F>
+__device__ __forceinline__ void fe_sub_p(uint32_t a[8], const F& f) {
+  asm("sub.cc.u32 %0, %0, %8;\n\t"
+      "subc.cc.u32 %1, %1, %9;\n\t"
+      "subc.cc.u32 %2, %2, %10;\n\t"
+      "subc.cc.u32 %3, %3, %11;\n\t"
+      "subc.cc.u32 %4, %4, %12;\n\t"
+      "subc.cc.u32 %5, %5, %13;\n\t"
+      "subc.cc.u32 %6, %6, %14;\n\t"
+      "subc.u32 %7, %7, %15;"
+      : "+r"(a[0]), "+r"(a[1]), "+r"(a[2]), "+r"(a[3]), "+r"(a[4]), "+r"(a[5]), "+r"(a[6]), "+r"(a[7])
+      : "r"(f.p(0)), "r"(f.p(1)), "r"(f.p(2)), "r"(f.p(3)), "r"(f.p(4)), "r"(f.p(5)), "r"(f.p(6)),
+        "r"(f.p(7)));
+}
+
+// Reduce any 256-bit value into [0, p) by repeated subtraction. For BN254
+// (p > 2^253) at most five subtractions are needed; for a general modulus the
+// caller reduces on the host instead.
+template <class F>
+__device__ __forceinline__ void fe_reduce_full(uint32_t a[8], const F& f, int max_sub) {
+  for (int k = 0; k < max_sub; ++k) {
+    if (fe_lt_p(a, f)) break;
+    fe_sub_p(a, f);
+  }
+}
+
+}  // namespace zkb

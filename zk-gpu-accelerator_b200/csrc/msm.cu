@@ -1,0 +1,535 @@
+// msm.cu — Pippenger multi-scalar multiplication over BN254 G1, entirely on
+// the device, and its C ABI.
+//
+// Pipeline for sum_i s_i P_i (zkgpu/msm_gpu.py:1-35 describes the reference's
+// version; here every step, including the final combination, is on the GPU):
+//   1. digits    one thread per scalar: reduce mod r, recode into W signed
+//                w-bit digits d (|d| <= 2^(w-1)), and emit one (bucket, point)
+//                pair per nonzero digit: key = window * 2^(w-1) + |d| - 1,
+//                value = point index | sign << 31.
+//   2. sort      radix sort of the pairs by key (CUB onesweep), so every
+//                bucket's points are contiguous; zero digits carry the largest
+//                key and sort to the end.
+//   3. buckets   level 1: each thread adds a fixed run of K1 sorted pairs into
+//                XYZZ accumulators with mixed additions, so every thread does
+//                the same work however skewed the buckets are. A bucket wholly
+//                inside one thread's run is written out directly; a bucket
+//                that crosses a run boundary leaves partial sums in per-thread
+//                slots, which later levels merge the same way (full XYZZ
+//                additions) until every bucket is complete. No host sync.
+//   4. reduction sum_b (b + 1) B_b per window by running sums over segments of
+//                L buckets, recursively over the segment sums (below).
+//   5. finalize  Horner over the window sums (w doublings per window) and one
+//                inversion to affine (zkgpu/msm.py:156-169, curve.py:221-233).
+//
+// Window-sum recursion: for a segment t of L consecutive entries X_{tL+i},
+// running sums from the top give S_t = sum_i X_{tL+i} and
+// U_t = sum_i (i + delta) X_{tL+i}; then
+//   sum_b (b + delta) X_b = sum_t U_t + L * sum_t t S_t,
+// and the last term is the same problem on the L S_t with delta = 0.
+#include <cub/device/device_radix_sort.cuh>
+
+#include <vector>
+
+#include "curve.cuh"
+#include "field_host.h"
+#include "profile.h"
+
+namespace zkb {
+
+static constexpr int kMsmMaxWindow = 20;
+static constexpr int kAcc1PerThread = 64;   // K1: sorted pairs per level-1 thread
+static constexpr int kSlotPerThread = 32;   // K2: slots per merge thread
+static constexpr int kReduceLogL = 3;       // reduction segments of 8 entries
+static constexpr int kScalarBits = 254;     // r < 2^254
+
+static int num_windows(int w) { return (kScalarBits + 1 + w - 1) / w; }
+
+// ---------------------------------------------------------------------------
+// 1. digits
+// ---------------------------------------------------------------------------
+
+// Bits [lo, lo + w) of a 256-bit little-endian value (w <= 20 spans two limbs
+// at most).
+__device__ __forceinline__ uint32_t scalar_bits(const uint32_t s[8], int lo, int w) {
+  const int limb = lo >> 5, off = lo & 31;
+  uint64_t v = s[limb];
+  if (limb + 1 < 8) v |= (uint64_t)s[limb + 1] << 32;
+  return (uint32_t)(v >> off) & ((1u << w) - 1u);
+}
+
+__global__ void __launch_bounds__(256) k_msm_digits(const uint64_t* scalars, int64_t n, int w,
+                                                    int W, uint32_t none, uint32_t* keys,
+                                                    uint32_t* vals) {
+  FrP fr;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const uint32_t half = 1u << (w - 1);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    uint32_t s[8];
+    fe_load_nc(s, scalars + 4 * i);
+    fe_reduce_full(s, fr, 5);  // any 256-bit value -> [0, r)
+    uint32_t carry = 0;
+    for (int win = 0; win < W; ++win) {
+      const int lo = win * w;
+      uint32_t raw = (lo < 256 ? scalar_bits(s, lo, w > 256 - lo ? 256 - lo : w) : 0) + carry;
+      uint32_t mag, neg = 0;
+      if (win + 1 < W && raw > half) {
+        // raw - 2^w in [-(2^(w-1) - 1), -1], borrow 1 from the next window
+        mag = (1u << w) - raw;
+        neg = 1;
+        carry = 1;
+      } else {
+        mag = raw;
+        carry = 0;
+      }
+      const int64_t e = (int64_t)win * n + i;
+      if (mag == 0) {
+        keys[e] = none;
+        vals[e] = 0;
+      } else {
+        keys[e] = ((uint32_t)win << (w - 1)) | (mag - 1);
+        vals[e] = (uint32_t)i | (neg << 31);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 3. bucket accumulation
+// ---------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(256) k_xyzz_fill_identity(uint64_t* pts, int64_t count) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride) {
+    // ZZ = ZZZ = 0 marks the identity; X and Y are ignored then
+    const uint4 z = make_uint4(0, 0, 0, 0);
+    uint4* p = reinterpret_cast<uint4*>(pts + 16 * i);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) p[k] = z;
+  }
+}
+
+// Writes a finished run: straight to its bucket when the run lies wholly in
+// this thread's range, else into this thread's head slot (first run) or tail
+// slot (last run). A single run that is shared fills the head slot and puts an
+// identity with the same key in the tail slot, so the slots of one bucket stay
+// contiguous for the next level.
+struct RunSink {
+  uint64_t* buckets;
+  uint32_t* slot_keys;
+  uint64_t* slot_pts;
+  int64_t t;
+  uint32_t prev_key, next_key, none;
+
+  __device__ __forceinline__ void flush(uint32_t key, const Xyzz& acc, bool is_first,
+                                        bool is_last) const {
+    if (key == none) return;
+    const bool shared = (is_first && prev_key == key) || (is_last && next_key == key);
+    if (!shared) {
+      xyzz_store(buckets + 16 * (int64_t)key, acc);
+      return;
+    }
+    if (is_first) {
+      slot_keys[2 * t] = key;
+      xyzz_store(slot_pts + 16 * (2 * t), acc);
+      if (is_last) {
+        Xyzz id;
+        xyzz_set_identity(id);
+        slot_keys[2 * t + 1] = key;
+        xyzz_store(slot_pts + 16 * (2 * t + 1), id);
+      }
+    } else {
+      slot_keys[2 * t + 1] = key;
+      xyzz_store(slot_pts + 16 * (2 * t + 1), acc);
+    }
+  }
+};
+
+// Level 1: K1 sorted (key, value) pairs per thread, mixed additions of affine
+// input points.
+__global__ void __launch_bounds__(128) k_msm_acc_points(const uint64_t* points,
+                                                        const uint32_t* keys,
+                                                        const uint32_t* vals, int64_t E, int K,
+                                                        uint32_t none, uint64_t* buckets,
+                                                        uint32_t* slot_keys, uint64_t* slot_pts) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t T = (E + K - 1) / K;
+  if (t >= T) return;
+  const int64_t start = t * K;
+  const int64_t end = start + K < E ? start + K : E;
+  RunSink sink{buckets, slot_keys, slot_pts, t, start > 0 ? keys[start - 1] : none,
+               end < E ? keys[end] : none, none};
+  slot_keys[2 * t] = none;
+  slot_keys[2 * t + 1] = none;
+  uint32_t cur = keys[start];
+  bool first = true;
+  Xyzz acc;
+  xyzz_set_identity(acc);
+  for (int64_t e = start; e < end; ++e) {
+    const uint32_t k = keys[e];
+    if (k != cur) {
+      sink.flush(cur, acc, first, false);
+      first = false;
+      xyzz_set_identity(acc);
+      cur = k;
+    }
+    if (k == none) break;  // zero digits sort last: nothing after them
+    const uint32_t v = vals[e];
+    Aff q;
+    aff_load_nc(q, points + 8 * (int64_t)(v & 0x7fffffffu));
+    if (v >> 31) aff_neg(q);
+    xyzz_add_affine(acc, q);
+  }
+  if (cur != none) sink.flush(cur, acc, first, true);
+}
+
+// Levels 2+: K2 slots per thread, full XYZZ additions; slots without a key
+// (none) may sit anywhere between runs and are skipped.
+__global__ void __launch_bounds__(128) k_msm_acc_slots(const uint32_t* in_keys,
+                                                       const uint64_t* in_pts, int64_t M, int K,
+                                                       uint32_t none, uint64_t* buckets,
+                                                       uint32_t* slot_keys, uint64_t* slot_pts) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t T = (M + K - 1) / K;
+  if (t >= T) return;
+  const int64_t start = t * K;
+  const int64_t end = start + K < M ? start + K : M;
+  RunSink sink{buckets, slot_keys, slot_pts, t, start > 0 ? in_keys[start - 1] : none,
+               end < M ? in_keys[end] : none, none};
+  slot_keys[2 * t] = none;
+  slot_keys[2 * t + 1] = none;
+  uint32_t cur = in_keys[start];
+  bool first = true;
+  Xyzz acc;
+  xyzz_set_identity(acc);
+  for (int64_t e = start; e < end; ++e) {
+    const uint32_t k = in_keys[e];
+    if (k != cur) {
+      sink.flush(cur, acc, first, false);
+      first = false;
+      xyzz_set_identity(acc);
+      cur = k;
+    }
+    if (k == none) continue;
+    Xyzz q;
+    xyzz_load(q, in_pts + 16 * e);
+    xyzz_add(acc, acc, q);
+  }
+  sink.flush(cur, acc, first, true);
+}
+
+// ---------------------------------------------------------------------------
+// 4. window reduction
+// ---------------------------------------------------------------------------
+
+// One thread per (window, segment). X and U_in are [W][G_in]; outputs are
+// [W][G_in / L] (S scaled by L), or the window sums at the last level.
+__global__ void __launch_bounds__(128) k_msm_reduce(const uint64_t* X, const uint64_t* U_in,
+                                                    int64_t G_in, int lL, int delta, int W,
+                                                    uint64_t* S_out, uint64_t* U_out,
+                                                    int final_level) {
+  const int64_t L = 1ll << lL;
+  const int64_t G_out = final_level ? 1 : G_in >> lL;
+  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= (int64_t)W * G_out) return;
+  const int64_t win = gid / G_out, t = gid % G_out;
+  const int64_t base = win * G_in + t * L;
+  const int64_t len = final_level ? G_in : L;
+  Xyzz running, tot, x;
+  xyzz_set_identity(running);
+  xyzz_set_identity(tot);
+  for (int64_t i = len - 1; i >= 0; --i) {
+    xyzz_load(x, X + 16 * (base + i));
+    xyzz_add(running, running, x);
+    if (i > 0 || delta) xyzz_add(tot, tot, running);
+  }
+  if (U_in) {
+    for (int64_t i = 0; i < len; ++i) {
+      xyzz_load(x, U_in + 16 * (base + i));
+      xyzz_add(tot, tot, x);
+    }
+  }
+  xyzz_store(U_out + 16 * (win * G_out + t), tot);
+  if (!final_level) {
+    for (int k = 0; k < lL; ++k) xyzz_dbl(running, running);
+    xyzz_store(S_out + 16 * (win * G_out + t), running);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 5. finalize
+// ---------------------------------------------------------------------------
+
+// Horner from the top window: acc = 2^w acc + S_win; then affine x = X / ZZ,
+// y = Y / ZZZ with one inversion of ZZ ZZZ, as plain canonical values.
+__global__ void k_msm_finalize(const uint64_t* window_sums, int W, int w, uint64_t* result) {
+  G1F f;
+  Xyzz acc, s;
+  xyzz_load(acc, window_sums + 16 * (W - 1));
+  for (int win = W - 2; win >= 0; --win) {
+    for (int k = 0; k < w; ++k) xyzz_dbl(acc, acc);
+    xyzz_load(s, window_sums + 16 * win);
+    xyzz_add(acc, acc, s);
+  }
+  uint32_t x[8], y[8];
+  uint64_t flag = 0;
+  if (xyzz_is_identity(acc)) {
+    fe_zero(x);
+    fe_zero(y);
+    flag = 1;
+  } else {
+    uint32_t prod[8], inv[8], t[8];
+    fe_mul(prod, acc.zz, acc.zzz, f);
+    fe_inv(inv, prod, f);
+    fe_mul(t, inv, acc.zzz, f);  // 1 / ZZ
+    fe_mul(x, acc.x, t, f);
+    fe_mul(t, inv, acc.zz, f);   // 1 / ZZZ
+    fe_mul(y, acc.y, t, f);
+    fe_from_mont(x, x, f);
+    fe_from_mont(y, y, f);
+  }
+  fe_store(result, x);
+  fe_store(result + 4, y);
+  result[8] = flag;
+}
+
+__global__ void k_msm_identity_result(uint64_t* result) {
+  for (int k = 0; k < 8; ++k) result[k] = 0;
+  result[8] = 1;
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+
+int default_window(int64_t n) {
+  // argmin over w of windows * (cost of n mixed additions + 2^(w-1) buckets'
+  // share of the reduction), in units of field multiplications: 10 per mixed
+  // addition, about 42 per bucket in the running sums.
+  if (n <= 1) return 1;
+  int best_w = 1;
+  double best = 1e300;
+  for (int w = 1; w <= 16; ++w) {
+    const double cost = (double)num_windows(w) * (10.0 * (double)n + 42.0 * (double)(1ll << (w - 1)));
+    if (cost < best) {
+      best = cost;
+      best_w = w;
+    }
+  }
+  return best_w;
+}
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+struct MsmPlan {
+  int64_t n = 0;
+  int w = 0, W = 0, key_bits = 0;
+  uint32_t none = 0;
+  int64_t nb = 0;  // buckets per window
+  int64_t E = 0;   // sorted pairs
+  int64_t T1 = 0;  // level-1 threads
+  std::vector<int64_t> slot_levels;  // thread count of each merge level
+  size_t cub_bytes = 0;
+  // workspace offsets
+  size_t off_keys0, off_keys1, off_vals0, off_vals1, off_cub, off_buckets, off_slot_keys_a,
+      off_slot_pts_a, off_slot_keys_b, off_slot_pts_b, off_red_s0, off_red_u0, off_red_s1,
+      off_red_u1, off_wsum, total;
+};
+
+static int make_plan(int64_t n, int w, MsmPlan& p) {
+  p.n = n;
+  p.w = w;
+  p.W = num_windows(w);
+  p.nb = 1ll << (w - 1);
+  const int64_t keys_used = (int64_t)p.W * p.nb;
+  int bits = 1;
+  while ((1ll << bits) <= keys_used) ++bits;  // keys_used itself must fit below none
+  p.key_bits = bits;
+  p.none = (uint32_t)((1ull << bits) - 1);
+  p.E = (int64_t)p.W * n;
+  p.T1 = (p.E + kAcc1PerThread - 1) / kAcc1PerThread;
+  p.slot_levels.clear();
+  int64_t M = 2 * p.T1;
+  int64_t T = p.T1;
+  while (T > 1) {
+    T = (M + kSlotPerThread - 1) / kSlotPerThread;
+    p.slot_levels.push_back(T);
+    M = 2 * T;
+  }
+  // CUB's temporary storage for sorting E pairs (a size query; launches nothing)
+  cub::DoubleBuffer<uint32_t> kb(nullptr, nullptr), vb(nullptr, nullptr);
+  size_t cub_bytes = 0;
+  cudaError_t err = cub::DeviceRadixSort::SortPairs(nullptr, cub_bytes, kb, vb, (int)p.E, 0,
+                                                    p.key_bits, (cudaStream_t)0);
+  if (err != cudaSuccess) return check_cuda(err, "CUB sort size query");
+  p.cub_bytes = cub_bytes;
+
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    size_t at = off;
+    off += align256(bytes);
+    return at;
+  };
+  p.off_keys0 = take((size_t)p.E * 4);
+  p.off_keys1 = take((size_t)p.E * 4);
+  p.off_vals0 = take((size_t)p.E * 4);
+  p.off_vals1 = take((size_t)p.E * 4);
+  p.off_cub = take(p.cub_bytes);
+  p.off_buckets = take((size_t)p.W * p.nb * 128);
+  p.off_slot_keys_a = take((size_t)2 * p.T1 * 4);
+  p.off_slot_pts_a = take((size_t)2 * p.T1 * 128);
+  const int64_t second = p.slot_levels.empty() ? 1 : p.slot_levels[0];
+  p.off_slot_keys_b = take((size_t)2 * second * 4);
+  p.off_slot_pts_b = take((size_t)2 * second * 128);
+  const int64_t red = (int64_t)p.W * (p.nb >> kReduceLogL > 0 ? p.nb >> kReduceLogL : 1);
+  p.off_red_s0 = take((size_t)red * 128);
+  p.off_red_u0 = take((size_t)red * 128);
+  p.off_red_s1 = take((size_t)red * 128);
+  p.off_red_u1 = take((size_t)red * 128);
+  p.off_wsum = take((size_t)p.W * 128);
+  p.total = off;
+  return ZKB_OK;
+}
+
+static int run_msm(const uint64_t* points, const uint64_t* scalars, const MsmPlan& p,
+                   uint64_t* result, char* ws, cudaStream_t s) {
+  uint32_t* keys0 = reinterpret_cast<uint32_t*>(ws + p.off_keys0);
+  uint32_t* keys1 = reinterpret_cast<uint32_t*>(ws + p.off_keys1);
+  uint32_t* vals0 = reinterpret_cast<uint32_t*>(ws + p.off_vals0);
+  uint32_t* vals1 = reinterpret_cast<uint32_t*>(ws + p.off_vals1);
+  uint64_t* buckets = reinterpret_cast<uint64_t*>(ws + p.off_buckets);
+
+  // 1. digits
+  {
+    ProfSpan span("msm_digits", s);
+    k_msm_digits<<<grid_for(p.n, 256), 256, 0, s>>>(scalars, p.n, p.w, p.W, p.none, keys0, vals0);
+    ZKB_TRY(check_launch("msm digits"));
+  }
+
+  // 2. sort
+  cub::DoubleBuffer<uint32_t> kb(keys0, keys1), vb(vals0, vals1);
+  size_t cub_bytes = p.cub_bytes;
+  {
+    ProfSpan span("msm_sort", s);
+    ZKB_TRY(check_cuda(cub::DeviceRadixSort::SortPairs(ws + p.off_cub, cub_bytes, kb, vb, (int)p.E,
+                                                       0, p.key_bits, s),
+                       "msm sort"));
+  }
+  const uint32_t* skeys = kb.Current();
+  const uint32_t* svals = vb.Current();
+
+  // 3. buckets
+  const int64_t nbuckets = (int64_t)p.W * p.nb;
+  k_xyzz_fill_identity<<<grid_for(nbuckets, 256), 256, 0, s>>>(buckets, nbuckets);
+  ZKB_TRY(check_launch("msm bucket init"));
+  uint32_t* sk[2] = {reinterpret_cast<uint32_t*>(ws + p.off_slot_keys_a),
+                     reinterpret_cast<uint32_t*>(ws + p.off_slot_keys_b)};
+  uint64_t* sp[2] = {reinterpret_cast<uint64_t*>(ws + p.off_slot_pts_a),
+                     reinterpret_cast<uint64_t*>(ws + p.off_slot_pts_b)};
+  {
+    ProfSpan span("msm_acc_points", s);
+    const unsigned grid = (unsigned)((p.T1 + 127) / 128);
+    k_msm_acc_points<<<grid, 128, 0, s>>>(points, skeys, svals, p.E, kAcc1PerThread, p.none,
+                                          buckets, sk[0], sp[0]);
+    ZKB_TRY(check_launch("msm bucket accumulation"));
+  }
+  {
+    ProfSpan span("msm_acc_merge", s);
+    int cur = 0;
+    int64_t M = 2 * p.T1;
+    for (size_t lvl = 0; lvl < p.slot_levels.size(); ++lvl) {
+      const int64_t T = p.slot_levels[lvl];
+      const unsigned grid = (unsigned)((T + 127) / 128);
+      k_msm_acc_slots<<<grid, 128, 0, s>>>(sk[cur], sp[cur], M, kSlotPerThread, p.none, buckets,
+                                           sk[cur ^ 1], sp[cur ^ 1]);
+      ZKB_TRY(check_launch("msm bucket merge"));
+      cur ^= 1;
+      M = 2 * T;
+    }
+  }
+
+  // 4. window reduction
+  uint64_t* rs[2] = {reinterpret_cast<uint64_t*>(ws + p.off_red_s0),
+                     reinterpret_cast<uint64_t*>(ws + p.off_red_s1)};
+  uint64_t* ru[2] = {reinterpret_cast<uint64_t*>(ws + p.off_red_u0),
+                     reinterpret_cast<uint64_t*>(ws + p.off_red_u1)};
+  uint64_t* wsum = reinterpret_cast<uint64_t*>(ws + p.off_wsum);
+  {
+    ProfSpan span("msm_reduce", s);
+    const uint64_t* X = buckets;
+    const uint64_t* U = nullptr;
+    int64_t G = p.nb;
+    int delta = 1, r = 0;
+    const int64_t L = 1ll << kReduceLogL;
+    while (G > L) {
+      const int64_t G_out = G / L;
+      const int64_t threads = (int64_t)p.W * G_out;
+      k_msm_reduce<<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(X, U, G, kReduceLogL, delta,
+                                                                     p.W, rs[r], ru[r], 0);
+      ZKB_TRY(check_launch("msm window reduction"));
+      X = rs[r];
+      U = ru[r];
+      r ^= 1;
+      G = G_out;
+      delta = 0;
+    }
+    k_msm_reduce<<<(unsigned)((p.W + 127) / 128), 128, 0, s>>>(X, U, G, kReduceLogL, delta, p.W,
+                                                               nullptr, wsum, 1);
+    ZKB_TRY(check_launch("msm window sums"));
+  }
+
+  // 5. finalize
+  ProfSpan fin_span("msm_finalize", s);
+  k_msm_finalize<<<1, 1, 0, s>>>(wsum, p.W, p.w, result);
+  return check_launch("msm finalize");
+}
+
+}  // namespace zkb
+
+using namespace zkb;
+
+extern "C" {
+
+int zkb_msm_default_window(int64_t n) { return zkb::default_window(n); }
+
+size_t zkb_msm_workspace_bytes(int64_t n, int window_size) {
+  set_error("%s", "");
+  if (n <= 0) return 0;
+  const int w = window_size ? window_size : default_window(n);
+  if (w < 1 || w > kMsmMaxWindow) return 0;
+  MsmPlan p;
+  if (make_plan(n, w, p) != ZKB_OK) return 0;
+  return p.total;
+}
+
+int zkb_msm(const uint64_t* points, const uint64_t* scalars, int64_t n, int window_size,
+            uint64_t* result, void* workspace, size_t workspace_bytes, void* stream) {
+  set_error("%s", "");
+  if (n < 0) return fail(ZKB_EINVAL, "negative point count");
+  if (n >= (1ll << 31)) return fail(ZKB_EINVAL, "at most 2^31 - 1 points per MSM");
+  if (window_size < 0 || window_size > kMsmMaxWindow) {
+    return fail(ZKB_EINVAL, "window_size must be in 1..%d (or 0 for the default), got %d",
+                kMsmMaxWindow, window_size);
+  }
+  if (!result) return fail(ZKB_EINVAL, "null result buffer");
+  cudaStream_t s = as_stream(stream);
+  if (n == 0) {
+    k_msm_identity_result<<<1, 1, 0, s>>>(result);
+    return check_launch("msm identity");
+  }
+  if (!points || !scalars) return fail(ZKB_EINVAL, "null buffer");
+  const int w = window_size ? window_size : default_window(n);
+  MsmPlan p;
+  ZKB_TRY(make_plan(n, w, p));
+  if ((int64_t)p.E >= (1ll << 31)) {
+    return fail(ZKB_EINVAL, "%lld points at window %d exceed the sort's 2^31 pairs",
+                (long long)n, w);
+  }
+  if (!workspace || workspace_bytes < p.total) {
+    return fail(ZKB_EWORKSPACE, "MSM of %lld points at window %d needs %zu workspace bytes, got %zu",
+                (long long)n, w, p.total, workspace_bytes);
+  }
+  return run_msm(points, scalars, p, result, reinterpret_cast<char*>(workspace), s);
+}
+
+}  // extern "C"

@@ -1,0 +1,600 @@
+// ntt.cu — natural-order radix-2 NTT over a 256-bit prime field, fused across
+// stages, and its C ABI.
+//
+// Transform (zkgpu/ntt.py:149-203, zkgpu/field256_gpu.py:347-387):
+//   forward  X[k] = sum_j x[j] w^(jk)            inverse  x[j] = n^-1 sum_k X[k] w^(-jk)
+// with the coset forms of zkgpu/domain.py:122-135 (x[j] scaled by g^j before a
+// forward transform, the result scaled by g^-j after an inverse one).
+//
+// Decomposition (four-step / Bailey): n = R_1 R_2 ... R_P with every R_q <= 4096.
+// Pass q transforms digit q of the index (stride S_q = R_{q+1} ... R_P) for
+// every fixed value of the other digits, then multiplies by the twiddle
+// w_B^(j' k) of its sub-problem (B = R_q S_q, j' the lower digits, k the new
+// frequency). The last pass writes X in natural order: position
+// sum_q k_q S_q holds X[sum_q k_q R_1 ... R_{q-1}].
+//
+// Each CTA stages C columns of one pass (C * R <= 4096 elements = 128 KiB) in
+// shared memory, bit-reverses them on the way in, runs all log2 R radix-2 DIT
+// stages there (one Montgomery multiplication per butterfly), and applies the
+// pass twiddle (and, for the first/last pass, the coset or n^-1 scaling) on
+// the way out: one HBM read and one HBM write per element per pass.
+#include <mutex>
+#include <list>
+#include <vector>
+#include <cstring>
+
+#include "field_host.h"
+#include "profile.h"
+
+namespace zkb {
+
+static constexpr int kMaxLogR = 12;                 // largest sub-transform: 4096 points
+static constexpr int kMaxCtaElems = 1 << kMaxLogR;  // elements staged per CTA
+static constexpr int kNttThreads = 512;
+static constexpr int kMaxLogN = 28;
+
+// w_{2^28} = 5^((r - 1) / 2^28) for BN254 Fr: the root every size derives from
+// (zkgpu/ntt.py:74-124; snarkjs's w[28], tests/test_domain.py:15).
+static const uint64_t kFrRoot28[4] = {0x9bd61b6e725b19f0ull, 0x402d111e41112ed4ull,
+                                      0x00e0a7eb8ef62abcull, 0x2a3c09f0a58a7e85ull};
+
+// ---------------------------------------------------------------------------
+// Tables
+// ---------------------------------------------------------------------------
+
+// Root tables for w_N (N = 2^log_N): w_N^e = t_lo[e & (2^s - 1)] * t_hi[e >> s];
+// stage tables w_fwd[j] = w_Rmax^j and w_inv[j] = w_Rmax^-j for j < Rmax / 2.
+struct RootTables {
+  uint64_t* t_lo = nullptr;
+  uint64_t* t_hi = nullptr;
+  uint64_t* w_fwd = nullptr;
+  uint64_t* w_inv = nullptr;
+  int log_N = 0, s = 0, log_rmax = 0;
+};
+
+// Per-transform scaling tables: forward coset: g^j = g_lo[j & m] g_hi[j >> gs];
+// inverse: n^-1 g^-j (g = 1 without a coset, then only `scale` = n^-1 is used).
+struct ScaleTables {
+  uint64_t* g_lo = nullptr;
+  uint64_t* g_hi = nullptr;
+  uint64_t* scale = nullptr;  // one element: n^-1 (Montgomery)
+  int gs = 0;
+};
+
+template <class F>
+__device__ __forceinline__ void fe_pow64(uint32_t r[8], const uint32_t base[8], uint64_t e,
+                                         const F& f) {
+  uint32_t acc[8], b[8];
+  fe_one(acc, f);
+  fe_copy(b, base);
+  while (e) {
+    if (e & 1) fe_mul(acc, acc, b, f);
+    e >>= 1;
+    if (e) fe_sqr(b, b, f);
+  }
+  fe_copy(r, acc);
+}
+
+// bases[0] = w (Montgomery), bases[1] = w^(2^s), bases[2] = w_Rmax = w^(N / Rmax),
+// bases[3] = w_Rmax^-1 = w_Rmax^(Rmax - 1).
+template <class F>
+__global__ void k_root_bases(F f, const uint64_t* omega_plain, uint64_t* bases, int log_N, int s,
+                             int log_rmax) {
+  uint32_t w[8], t[8];
+  fe_load(t, omega_plain);
+  fe_to_mont(w, t, f);
+  fe_store(bases, w);
+  fe_pow64(t, w, 1ull << s, f);
+  fe_store(bases + 4, t);
+  uint32_t wr[8];
+  fe_pow64(wr, w, 1ull << (log_N - log_rmax), f);
+  fe_store(bases + 8, wr);
+  fe_pow64(t, wr, (1ull << log_rmax) - 1, f);
+  fe_store(bases + 12, t);
+}
+
+// out[i] = pre * base^i for i < count (pre = 1 when null).
+template <class F>
+__global__ void k_pow_table(F f, const uint64_t* base, const uint64_t* pre, uint64_t* out,
+                            int64_t count) {
+  uint32_t b[8], r[8];
+  fe_load(b, base);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride) {
+    fe_pow64(r, b, (uint64_t)i, f);
+    if (pre) {
+      uint32_t p[8];
+      fe_load(p, pre);
+      fe_mul(r, r, p, f);
+    }
+    fe_store(out + 4 * i, r);
+  }
+}
+
+// Scaling bases: g (Montgomery) or g^-1, g^(+-2^gs), and n^-1.
+// out: [0] = step base for g_lo, [1] = step base for g_hi, [2] = n^-1, [3] = pre
+// for g_hi (n^-1 for inverse transforms, 1 for forward ones).
+template <class F>
+__global__ void k_scale_bases(F f, const uint64_t* g_plain, int has_coset, int inverse,
+                              int64_t n, int gs, uint64_t* out) {
+  uint32_t g[8], t[8], ninv[8], one[8];
+  fe_one(one, f);
+  // n as a field element (n < 2^29 fits a limb; reduce for tiny moduli)
+  uint32_t nv[8] = {(uint32_t)n, 0, 0, 0, 0, 0, 0, 0};
+  fe_reduce_full(nv, f, 64);
+  fe_to_mont(t, nv, f);
+  fe_inv(ninv, t, f);
+  fe_store(out + 8, ninv);
+  if (has_coset) {
+    fe_load(t, g_plain);
+    fe_to_mont(g, t, f);
+    if (inverse) fe_inv(g, g, f);
+    fe_store(out, g);
+    fe_pow64(t, g, 1ull << gs, f);
+    fe_store(out + 4, t);
+  } else {
+    fe_store(out, one);
+    fe_store(out + 4, one);
+  }
+  fe_store(out + 12, inverse ? ninv : one);
+}
+
+struct TableKey {
+  uint64_t modulus[4];
+  uint64_t omega[4];
+  int log_N;
+  int device;
+  bool operator==(const TableKey& o) const {
+    return std::memcmp(modulus, o.modulus, sizeof modulus) == 0 &&
+           std::memcmp(omega, o.omega, sizeof omega) == 0 && log_N == o.log_N &&
+           device == o.device;
+  }
+};
+
+struct ScaleKey {
+  TableKey root;
+  uint64_t g[4];
+  int has_coset, inverse;
+  int64_t n;
+  bool operator==(const ScaleKey& o) const {
+    return root == o.root && std::memcmp(g, o.g, sizeof g) == 0 && has_coset == o.has_coset &&
+           inverse == o.inverse && n == o.n;
+  }
+};
+
+struct RootEntry {
+  TableKey key;
+  RootTables t;
+  void* mem;
+};
+struct ScaleEntry {
+  ScaleKey key;
+  ScaleTables t;
+  void* mem;
+};
+
+static std::mutex g_ntt_mutex;
+static std::list<RootEntry> g_roots;    // most recently used first
+static std::list<ScaleEntry> g_scales;  // most recently used first
+static constexpr size_t kMaxRootEntries = 16;  // like the reference's lru_cache(16)
+static constexpr size_t kMaxScaleEntries = 64;
+
+template <class F>
+static int build_roots(const F& f, const TableKey& key, RootTables& t, void** mem,
+                       cudaStream_t s) {
+  t.log_N = key.log_N;
+  t.s = (key.log_N + 1) / 2;
+  t.log_rmax = key.log_N < kMaxLogR ? key.log_N : kMaxLogR;
+  const int64_t n_lo = 1ll << t.s, n_hi = 1ll << (key.log_N - t.s);
+  const int64_t n_w = t.log_rmax > 0 ? (1ll << (t.log_rmax - 1)) : 1;
+  const size_t elems = (size_t)(n_lo + n_hi + 2 * n_w + 4 + 1 /* omega */);
+  uint64_t* base = nullptr;
+  ZKB_TRY(check_cuda(cudaMalloc(&base, elems * 32), "NTT root table allocation"));
+  *mem = base;
+  t.t_lo = base;
+  t.t_hi = t.t_lo + 4 * n_lo;
+  t.w_fwd = t.t_hi + 4 * n_hi;
+  t.w_inv = t.w_fwd + 4 * n_w;
+  uint64_t* bases = t.w_inv + 4 * n_w;
+  uint64_t* omega_dev = bases + 16;
+  ZKB_TRY(check_cuda(cudaMemcpyAsync(omega_dev, key.omega, 32, cudaMemcpyHostToDevice, s),
+                     "NTT root upload"));
+  k_root_bases<<<1, 1, 0, s>>>(f, omega_dev, bases, key.log_N, t.s, t.log_rmax);
+  ZKB_TRY(check_launch("NTT root bases"));
+  k_pow_table<<<grid_for(n_lo, 128), 128, 0, s>>>(f, bases, nullptr, t.t_lo, n_lo);
+  ZKB_TRY(check_launch("NTT root table (low powers)"));
+  k_pow_table<<<grid_for(n_hi, 128), 128, 0, s>>>(f, bases + 4, nullptr, t.t_hi, n_hi);
+  ZKB_TRY(check_launch("NTT root table (high powers)"));
+  k_pow_table<<<grid_for(n_w, 128), 128, 0, s>>>(f, bases + 8, nullptr, t.w_fwd, n_w);
+  ZKB_TRY(check_launch("NTT stage table"));
+  k_pow_table<<<grid_for(n_w, 128), 128, 0, s>>>(f, bases + 12, nullptr, t.w_inv, n_w);
+  ZKB_TRY(check_launch("NTT inverse stage table"));
+  // Other streams may use the entry as soon as it is published.
+  return check_cuda(cudaStreamSynchronize(s), "NTT root table build");
+}
+
+template <class F>
+static int build_scale(const F& f, const ScaleKey& key, int log_n, ScaleTables& t, void** mem,
+                       cudaStream_t s) {
+  t.gs = (log_n + 1) / 2;
+  const int64_t n_lo = 1ll << t.gs, n_hi = 1ll << (log_n - t.gs);
+  const bool tables = key.has_coset != 0;
+  const size_t elems = (size_t)((tables ? n_lo + n_hi : 0) + 4 + 1);
+  uint64_t* base = nullptr;
+  ZKB_TRY(check_cuda(cudaMalloc(&base, elems * 32), "NTT scale table allocation"));
+  *mem = base;
+  uint64_t* bases = base + (tables ? 4 * (n_lo + n_hi) : 0);
+  uint64_t* g_dev = bases + 16;
+  t.scale = bases + 8;
+  ZKB_TRY(check_cuda(cudaMemcpyAsync(g_dev, key.g, 32, cudaMemcpyHostToDevice, s),
+                     "NTT coset upload"));
+  k_scale_bases<<<1, 1, 0, s>>>(f, g_dev, key.has_coset, key.inverse, key.n, t.gs, bases);
+  ZKB_TRY(check_launch("NTT scale bases"));
+  if (tables) {
+    t.g_lo = base;
+    t.g_hi = base + 4 * n_lo;
+    k_pow_table<<<grid_for(n_lo, 128), 128, 0, s>>>(f, bases, nullptr, t.g_lo, n_lo);
+    ZKB_TRY(check_launch("NTT coset table (low powers)"));
+    k_pow_table<<<grid_for(n_hi, 128), 128, 0, s>>>(f, bases + 4, bases + 12, t.g_hi, n_hi);
+    ZKB_TRY(check_launch("NTT coset table (high powers)"));
+  }
+  return check_cuda(cudaStreamSynchronize(s), "NTT scale table build");
+}
+
+// ---------------------------------------------------------------------------
+// The pass kernel
+// ---------------------------------------------------------------------------
+
+struct NttPass {
+  const uint64_t* in;
+  uint64_t* out;
+  int lr, ls, lc;       // log2 of: sub-transform size R, element stride S, columns per CTA C
+  int last, first, inverse;
+  int lR1, lR2;         // last pass: output index = (o >> lR2) + ((o & (R2-1)) << lR1) + k * (n / R)
+  int log_n;
+  // tables
+  const uint64_t* t_lo;
+  const uint64_t* t_hi;
+  const uint64_t* w;    // stage table for this direction (w_Rmax^(+-j))
+  int s, log_N, log_rmax;
+  const uint64_t* g_lo; // coset tables (null without a coset)
+  const uint64_t* g_hi;
+  int gs;
+  const uint64_t* scale;  // n^-1 for an inverse transform without coset tables
+};
+
+// Shared-memory address (in uint64 units) of element j of column c: columns
+// are padded by 16 bytes so that consecutive columns start in different banks.
+__device__ __forceinline__ int sm_index(int c, int j, int lr) {
+  return c * ((4 << lr) + 2) + 4 * j;
+}
+
+template <class F>
+__device__ __forceinline__ void root_power(uint32_t r[8], const NttPass& a, uint64_t e, const F& f) {
+  // w_N^e for 0 <= e < N
+  const uint64_t mask = (1ull << a.s) - 1;
+  uint32_t lo[8], hi[8];
+  fe_load_nc(lo, a.t_lo + 4 * (e & mask));
+  fe_load_nc(hi, a.t_hi + 4 * (e >> a.s));
+  fe_mul(r, lo, hi, f);
+}
+
+template <class F>
+__global__ void __launch_bounds__(kNttThreads, 1) k_ntt_pass(F f, NttPass a) {
+  extern __shared__ uint4 smem_raw[];
+  uint64_t* sm = reinterpret_cast<uint64_t*>(smem_raw);
+  const int lr = a.lr, lc = a.lc;
+  const int R = 1 << lr, C = 1 << lc;
+  const int total = C << lr;
+  const int64_t S = 1ll << a.ls;
+  const int64_t B = (int64_t)R << a.ls;
+  const int64_t bid = blockIdx.x;
+
+  // Column bases.
+  //   non-last: o = bid / (S / C), first inner index j0 = (bid % (S / C)) * C,
+  //             element (c, j) at position o B + j S + j0 + c.
+  //   last:     k2 = bid % R2, k1_0 = (bid / R2) C; row o_c = (k1_0 + c) R2 + k2,
+  //             element (c, j) at position o_c R + j.
+  int64_t o = 0, j0 = 0, k2 = 0, k1_0 = 0;
+  if (!a.last) {
+    const int64_t groups = S >> lc;
+    o = bid / groups;
+    j0 = (bid % groups) << lc;
+  } else {
+    const int64_t R2 = 1ll << a.lR2;
+    k2 = bid & (R2 - 1);
+    k1_0 = (bid >> a.lR2) << lc;
+  }
+
+  // ---- load (bit-reversed into shared memory), with the coset pre-scale ----
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    int c, j;
+    int64_t pos;
+    if (!a.last) {
+      c = t & (C - 1);
+      j = t >> lc;
+      pos = o * B + (int64_t)j * S + j0 + c;
+    } else {
+      c = t >> lr;
+      j = t & (R - 1);
+      pos = (((k1_0 + c) << a.lR2) + k2) * R + j;
+    }
+    uint32_t x[8];
+    fe_load_nc(x, a.in + 4 * pos);
+    if (a.first && a.g_lo && !a.inverse) {
+      const uint64_t m = (1ull << a.gs) - 1;
+      uint32_t lo[8], hi[8];
+      fe_load_nc(lo, a.g_lo + 4 * ((uint64_t)pos & m));
+      fe_load_nc(hi, a.g_hi + 4 * ((uint64_t)pos >> a.gs));
+      fe_mul(lo, lo, hi, f);
+      fe_mul(x, x, lo, f);
+    }
+    const int jr = lr ? (int)(__brev((unsigned)j) >> (32 - lr)) : 0;
+    fe_store(sm + sm_index(c, jr, lr), x);
+  }
+  __syncthreads();
+
+  // ---- radix-2 DIT stages in shared memory ----
+  const int half_total = total >> 1;
+  for (int st = 0; st < lr; ++st) {
+    const int half = 1 << st;
+    for (int b = threadIdx.x; b < half_total; b += blockDim.x) {
+      const int c = b >> (lr - 1);
+      const int k = b & ((R >> 1) - 1);
+      const int jj = k & (half - 1);
+      const int i0 = ((k >> st) << (st + 1)) | jj;
+      const int i1 = i0 + half;
+      uint32_t u[8], v[8], w[8];
+      fe_load(u, sm + sm_index(c, i0, lr));
+      fe_load(v, sm + sm_index(c, i1, lr));
+      fe_load_nc(w, a.w + 4 * ((int64_t)jj << (a.log_rmax - 1 - st)));
+      fe_mul(v, v, w, f);
+      uint32_t x[8];
+      fe_add(x, u, v, f);
+      fe_sub(v, u, v, f);
+      fe_store(sm + sm_index(c, i0, lr), x);
+      fe_store(sm + sm_index(c, i1, lr), v);
+    }
+    __syncthreads();
+  }
+
+  // ---- store, with the pass twiddle or the final scaling ----
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    const int c = t & (C - 1);
+    const int k = t >> lc;
+    uint32_t x[8];
+    fe_load(x, sm + sm_index(c, k, lr));
+    if (!a.last) {
+      // w_B^((j0 + c) k) = w_N^((j0 + c) k N / B); inverse uses w_N^-e = w_N^(N - e)
+      const int64_t jp = j0 + c;
+      uint64_t e = ((uint64_t)(jp * k)) << (a.log_N - (lr + a.ls));
+      if (a.inverse && e) e = (1ull << a.log_N) - e;
+      if (e) {
+        uint32_t tw[8];
+        root_power(tw, a, e, f);
+        fe_mul(x, x, tw, f);
+      }
+      const int64_t pos = o * B + (int64_t)k * S + jp;
+      fe_store(a.out + 4 * pos, x);
+    } else {
+      const int64_t oc = ((k1_0 + c) << a.lR2) + k2;
+      const int64_t outidx = (oc >> a.lR2) + ((oc & ((1ll << a.lR2) - 1)) << a.lR1) +
+                             ((int64_t)k << (a.log_n - lr));
+      if (a.inverse) {
+        uint32_t sc[8];
+        if (a.g_lo) {
+          const uint64_t m = (1ull << a.gs) - 1;
+          uint32_t lo[8], hi[8];
+          fe_load_nc(lo, a.g_lo + 4 * ((uint64_t)outidx & m));
+          fe_load_nc(hi, a.g_hi + 4 * ((uint64_t)outidx >> a.gs));
+          fe_mul(sc, lo, hi, f);
+        } else {
+          fe_load_nc(sc, a.scale);
+        }
+        fe_mul(x, x, sc, f);
+      }
+      fe_store(a.out + 4 * outidx, x);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+
+static int ilog2(int64_t n) {
+  int l = 0;
+  while ((1ll << l) < n) ++l;
+  return l;
+}
+
+size_t workspace_bytes(int64_t n) {
+  if (n <= (1ll << kMaxLogR)) return 0;
+  return (size_t)n * 32;
+}
+
+// Splits log_n into P parts of at most kMaxLogR bits, the larger parts first.
+static std::vector<int> plan_radices(int log_n) {
+  const int P = (log_n + kMaxLogR - 1) / kMaxLogR;
+  std::vector<int> r(P, log_n / P);
+  for (int q = 0; q < log_n % P; ++q) r[q] += 1;
+  return r;
+}
+
+template <class F>
+static int run_ntt(const F& f, const zkb_field* field, const uint64_t* in, uint64_t* out,
+                   int64_t n, int invert, const uint64_t* omega, const uint64_t* coset,
+                   void* workspace, size_t ws_bytes, cudaStream_t s) {
+  const int log_n = ilog2(n);
+  TableKey key;
+  std::memcpy(key.modulus, field->modulus, sizeof key.modulus);
+  if (omega) {
+    std::memcpy(key.omega, omega, sizeof key.omega);
+    key.log_N = log_n;
+  } else {
+    std::memcpy(key.omega, kFrRoot28, sizeof key.omega);
+    key.log_N = kMaxLogN;
+  }
+  ZKB_TRY(check_cuda(cudaGetDevice(&key.device), "cudaGetDevice"));
+
+  RootTables rt;
+  ScaleTables st;
+  {
+    std::lock_guard<std::mutex> lock(g_ntt_mutex);
+    auto it = g_roots.begin();
+    for (; it != g_roots.end(); ++it)
+      if (it->key == key) break;
+    if (it == g_roots.end()) {
+      RootEntry e;
+      e.key = key;
+      e.mem = nullptr;
+      int rc = build_roots(f, key, e.t, &e.mem, s);
+      if (rc != ZKB_OK) {
+        if (e.mem) cudaFree(e.mem);
+        return rc;
+      }
+      g_roots.push_front(e);
+      if (g_roots.size() > kMaxRootEntries) {
+        // kernels queued on any stream may still read the evicted tables
+        cudaDeviceSynchronize();
+        cudaFree(g_roots.back().mem);
+        g_roots.pop_back();
+      }
+    } else {
+      g_roots.splice(g_roots.begin(), g_roots, it);
+    }
+    rt = g_roots.front().t;
+
+    if (invert || coset) {
+      ScaleKey sk;
+      sk.root = key;
+      std::memset(sk.g, 0, sizeof sk.g);
+      if (coset) std::memcpy(sk.g, coset, sizeof sk.g);
+      sk.has_coset = coset != nullptr;
+      sk.inverse = invert;
+      sk.n = n;
+      auto jt = g_scales.begin();
+      for (; jt != g_scales.end(); ++jt)
+        if (jt->key == sk) break;
+      if (jt == g_scales.end()) {
+        ScaleEntry e;
+        e.key = sk;
+        e.mem = nullptr;
+        int rc = build_scale(f, sk, log_n, e.t, &e.mem, s);
+        if (rc != ZKB_OK) {
+          if (e.mem) cudaFree(e.mem);
+          return rc;
+        }
+        g_scales.push_front(e);
+        if (g_scales.size() > kMaxScaleEntries) {
+          cudaDeviceSynchronize();
+          cudaFree(g_scales.back().mem);
+          g_scales.pop_back();
+        }
+      } else {
+        g_scales.splice(g_scales.begin(), g_scales, jt);
+      }
+      st = g_scales.front().t;
+    }
+  }
+
+  const std::vector<int> radices = plan_radices(log_n);
+  const int P = (int)radices.size();
+  uint64_t* tmp = P > 1 ? reinterpret_cast<uint64_t*>(workspace) : nullptr;
+  if (P > 1 && (!workspace || ws_bytes < workspace_bytes(n))) {
+    return fail(ZKB_EWORKSPACE, "NTT of %lld rows needs %zu workspace bytes, got %zu",
+                (long long)n, workspace_bytes(n), ws_bytes);
+  }
+
+  int ls = log_n;  // stride exponent of the current pass: S_q = 2^(log_n - sum of radices so far)
+  for (int q = 0; q < P; ++q) {
+    NttPass a;
+    std::memset(&a, 0, sizeof a);
+    a.lr = radices[q];
+    ls -= a.lr;
+    a.ls = ls;
+    a.last = q == P - 1;
+    a.first = q == 0;
+    a.inverse = invert;
+    a.log_n = log_n;
+    a.in = q == 0 ? in : tmp;
+    a.out = a.last ? out : tmp;
+    a.t_lo = rt.t_lo;
+    a.t_hi = rt.t_hi;
+    a.w = invert ? rt.w_inv : rt.w_fwd;
+    a.s = rt.s;
+    a.log_N = rt.log_N;
+    a.log_rmax = rt.log_rmax;
+    a.g_lo = st.g_lo;
+    a.g_hi = st.g_hi;
+    a.gs = st.gs;
+    a.scale = st.scale;
+    int lc;
+    int64_t ctas;
+    if (!a.last) {
+      lc = kMaxLogR - a.lr;
+      if (lc > a.ls) lc = a.ls;
+      ctas = n >> (a.lr + lc);
+    } else {
+      // R1 = first radix, R2 = product of the middle radices (P = 3 at most
+      // for n <= 2^28 with 4096-point passes, so R2 is radices[1] then).
+      const int lR1 = radices[0];
+      const int lR2 = P >= 3 ? radices[1] : 0;
+      a.lR1 = P >= 2 ? lR1 : 0;
+      a.lR2 = lR2;
+      lc = kMaxLogR - a.lr;
+      const int k1_bits = P >= 2 ? lR1 : 0;
+      if (lc > k1_bits) lc = k1_bits;
+      ctas = n >> (a.lr + lc);
+    }
+    a.lc = lc;
+    const size_t smem = (size_t)(1 << lc) * ((32u << a.lr) + 16);
+    auto kern = k_ntt_pass<F>;
+    ZKB_TRY(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)smem),
+                       "NTT shared memory attribute"));
+    int threads = kNttThreads;
+    const int half_total = (1 << (a.lr + lc)) >> 1;
+    if (half_total < threads) threads = half_total < 32 ? 32 : half_total;
+    {
+      ProfSpan span(a.last ? (q == 0 ? "ntt_single_pass" : "ntt_last_pass") : "ntt_column_pass", s);
+      kern<<<(unsigned)ctas, threads, smem, s>>>(f, a);
+      ZKB_TRY(check_launch("NTT pass launch"));
+    }
+  }
+  return ZKB_OK;
+}
+
+}  // namespace zkb
+
+using namespace zkb;
+
+extern "C" {
+
+size_t zkb_ntt_workspace_bytes(int64_t n) { return zkb::workspace_bytes(n); }
+
+int zkb_ntt(const zkb_field* f, const uint64_t* in, uint64_t* out, int64_t n, int invert,
+            const uint64_t* omega, const uint64_t* coset, void* workspace,
+            size_t workspace_bytes, void* stream) {
+  set_error("%s", "");
+  ZKB_TRY(check_field(f));
+  if (n < 0 || (n & (n - 1)) || n > (1ll << kMaxLogN)) {
+    return fail(ZKB_EINVAL, "NTT length must be a power of 2 up to 2^28, got %lld", (long long)n);
+  }
+  if (n == 0) return ZKB_OK;
+  if (!in || !out) return fail(ZKB_EINVAL, "null buffer");
+  if (in == out) return fail(ZKB_EINVAL, "NTT output must not alias its input");
+  if (!omega && f->kind != ZKB_FIELD_BN254_FR) {
+    return fail(ZKB_EINVAL, "a root of unity is required for fields other than BN254 Fr");
+  }
+  cudaStream_t s = as_stream(stream);
+  if (n == 1) {
+    // a single value transforms to itself; n^-1 = 1 and g^0 = 1
+    return check_cuda(cudaMemcpyAsync(out, in, 32, cudaMemcpyDeviceToDevice, s), "NTT copy");
+  }
+  return with_field(f, [&](auto fp) {
+    return run_ntt(fp, f, in, out, n, invert, omega, coset, workspace, workspace_bytes, s);
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,124 @@
+// runtime.cu — error reporting, version, and the host side of field set-up.
+#include <atomic>
+#include <cstring>
+
+#include "common.cuh"
+#include "field_host.h"
+
+namespace zkb {
+
+static thread_local char g_last_error[1024] = "";
+static std::atomic<unsigned long long> g_launches{0};
+
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+void set_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_last_error, sizeof g_last_error, fmt, ap);
+  va_end(ap);
+}
+
+// ---- 256-bit host helpers (little-endian uint64 limbs) ----------------------
+
+static bool u256_ge(const uint64_t a[4], const uint64_t b[4]) {
+  for (int j = 3; j >= 0; --j) {
+    if (a[j] != b[j]) return a[j] > b[j];
+  }
+  return true;
+}
+
+static void u256_sub(uint64_t r[4], const uint64_t a[4], const uint64_t b[4]) {
+  unsigned __int128 borrow = 0;
+  for (int j = 0; j < 4; ++j) {
+    unsigned __int128 d = (unsigned __int128)a[j] - b[j] - borrow;
+    r[j] = (uint64_t)d;
+    borrow = (d >> 64) ? 1 : 0;
+  }
+}
+
+// r = 2r mod p for r < p < 2^255 (2r < 2^256, no fifth limb needed).
+static void u256_double_mod(uint64_t r[4], const uint64_t p[4]) {
+  uint64_t carry = 0;
+  for (int j = 0; j < 4; ++j) {
+    uint64_t next = r[j] >> 63;
+    r[j] = (r[j] << 1) | carry;
+    carry = next;
+  }
+  if (u256_ge(r, p)) u256_sub(r, r, p);
+}
+
+static const uint64_t kBn254R[4] = {0x43e1f593f0000001ull, 0x2833e84879b97091ull,
+                                    0xb85045b68181585dull, 0x30644e72e131a029ull};
+static const uint64_t kBn254P[4] = {0x3c208c16d87cfd47ull, 0x97816a916871ca8dull,
+                                    0xb85045b68181585dull, 0x30644e72e131a029ull};
+
+int field_init(zkb_field* f, const uint64_t modulus[4]) {
+  if (!f || !modulus) return fail(ZKB_EINVAL, "zkb_field_init: null pointer");
+  // odd and in [3, 2^255) (zkgpu/field256_gpu.py:278-280)
+  bool small = modulus[3] == 0 && modulus[2] == 0 && modulus[1] == 0 && modulus[0] < 3;
+  if ((modulus[0] & 1) == 0 || small || (modulus[3] >> 63) != 0) {
+    return fail(ZKB_EINVAL, "modulus must be odd and in [3, 2^255)");
+  }
+  std::memset(f, 0, sizeof *f);
+  std::memcpy(f->modulus, modulus, sizeof f->modulus);
+  // R mod p: 1 doubled 256 times; R^2 mod p: 256 more doublings.
+  uint64_t r[4] = {1, 0, 0, 0};
+  if (u256_ge(r, modulus)) u256_sub(r, r, modulus);
+  for (int i = 0; i < 256; ++i) u256_double_mod(r, modulus);
+  std::memcpy(f->one, r, sizeof r);
+  for (int i = 0; i < 256; ++i) u256_double_mod(r, modulus);
+  std::memcpy(f->r2, r, sizeof r);
+  // p^-1 mod 2^64 by Newton's iteration (each step doubles the correct bits;
+  // x = p is already correct to 3 bits for odd p), then negate.
+  uint64_t x = modulus[0];
+  for (int i = 0; i < 6; ++i) x *= 2 - modulus[0] * x;
+  f->ninv = (uint64_t)0 - x;
+  if (std::memcmp(modulus, kBn254R, sizeof kBn254R) == 0) {
+    f->kind = ZKB_FIELD_BN254_FR;
+  } else if (std::memcmp(modulus, kBn254P, sizeof kBn254P) == 0) {
+    f->kind = ZKB_FIELD_BN254_FQ;
+  } else {
+    f->kind = ZKB_FIELD_GENERIC;
+  }
+  return ZKB_OK;
+}
+
+FieldRT to_rt(const zkb_field& f) {
+  FieldRT rt;
+  for (int j = 0; j < 4; ++j) {
+    rt.P[2 * j] = (uint32_t)f.modulus[j];
+    rt.P[2 * j + 1] = (uint32_t)(f.modulus[j] >> 32);
+    rt.ONE[2 * j] = (uint32_t)f.one[j];
+    rt.ONE[2 * j + 1] = (uint32_t)(f.one[j] >> 32);
+    rt.R2[2 * j] = (uint32_t)f.r2[j];
+    rt.R2[2 * j + 1] = (uint32_t)(f.r2[j] >> 32);
+  }
+  rt.NINV = (uint32_t)f.ninv;
+  return rt;
+}
+
+int check_field(const zkb_field* f) {
+  if (!f) return fail(ZKB_EINVAL, "null field");
+  if (f->kind != ZKB_FIELD_GENERIC && f->kind != ZKB_FIELD_BN254_FR && f->kind != ZKB_FIELD_BN254_FQ) {
+    return fail(ZKB_EINVAL, "field not initialised by zkb_field_init");
+  }
+  return ZKB_OK;
+}
+
+}  // namespace zkb
+
+extern "C" {
+
+const char* zkb_last_error(void) { return zkb::g_last_error; }
+
+int zkb_version(void) { return 100; }
+
+uint64_t zkb_launch_count(void) { return zkb::g_launches.load(); }
+
+int zkb_field_init(zkb_field* f, const uint64_t modulus[4]) {
+  zkb::set_error("%s", "");
+  return zkb::field_init(f, modulus);
+}
+
+}  // extern "C"
