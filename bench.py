@@ -244,7 +244,7 @@ class Step:
         self.msm_ws = torch.empty(self.msm_ws_bytes, dtype=torch.uint8, device="cuda")
         self.ntt_ws_bytes = int(self.lib.zkb_ntt_workspace_bytes(m))
         self.ntt_ws = torch.empty(max(self.ntt_ws_bytes, 1), dtype=torch.uint8, device="cuda")
-        self.result = torch.empty((2, 9), dtype=torch.int64, device="cuda")
+        self.result = torch.empty((2, 16), dtype=torch.int64, device="cuda")  # 128-byte rows
         self.coset = _native.u64_array(_native.limbs(COSET))
         torch.cuda.synchronize()
 

@@ -99,6 +99,11 @@ def test_gpu_entry_points_reject_bad_arguments_before_touching_the_device():
     assert lib.zkb_msm(8, 8, 10, 21, 8, None, 0, None) == _native.ZKB_EINVAL
     assert "window_size" in _native.last_error()
     assert lib.zkb_field_mul(ctypes.byref(f), 0, 1, 0, 1, 0, 0, None) == _native.ZKB_OK  # n = 0 is a no-op
+    # misaligned row buffers are refused on the host, before any launch
+    assert lib.zkb_field_mul(ctypes.byref(f), 8, 1, 32, 1, 64, 4, None) == _native.ZKB_EINVAL
+    assert "16-byte aligned" in _native.last_error()
+    assert lib.zkb_msm(64, 64, 4, 0, 4, None, 0, None) == _native.ZKB_EINVAL
+    assert "8-byte aligned" in _native.last_error()
 
 
 # ------------------------------------------------------------------

@@ -44,6 +44,16 @@ inline int check_launch(const char* what) {
 
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// Row buffers are read and written as 16-byte vectors: a buffer that is not
+// aligned is refused instead of faulting on the device. Null passes (callers
+// check for null separately where a buffer is required).
+inline int check_align(const void* p, unsigned align, const char* name) {
+  if (p && (reinterpret_cast<uintptr_t>(p) & (align - 1)) != 0) {
+    return fail(ZKB_EINVAL, "%s must be %u-byte aligned", name, align);
+  }
+  return ZKB_OK;
+}
+
 // Grid sizes: grid-stride loops over n items, at most `cap` blocks. The cap
 // is a multiple of the B200's 148 SMs.
 inline unsigned grid_for(int64_t n, int threads, int64_t cap = 148 * 64) {

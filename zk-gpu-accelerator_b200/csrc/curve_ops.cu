@@ -146,6 +146,9 @@ int zkb_g1_add(const uint64_t* a, int64_t a_step, const uint64_t* b, int64_t b_s
   ZKB_TRY(check_steps(n, a_step, b_step));
   if (n == 0) return ZKB_OK;
   if (!a || !b || !out) return fail(ZKB_EINVAL, "null buffer");
+  ZKB_TRY(check_align(a, 16, "a"));
+  ZKB_TRY(check_align(b, 16, "b"));
+  ZKB_TRY(check_align(out, 16, "out"));
   k_g1_add<<<grid_for(n, 128), 128, 0, as_stream(stream)>>>(a, a_step, b, b_step, out, n);
   return check_launch("g1_add launch");
 }
@@ -156,6 +159,9 @@ int zkb_g1_add_affine(const uint64_t* a, int64_t a_step, const uint64_t* b, int6
   ZKB_TRY(check_steps(n, a_step, b_step));
   if (n == 0) return ZKB_OK;
   if (!a || !b || !out) return fail(ZKB_EINVAL, "null buffer");
+  ZKB_TRY(check_align(a, 16, "a"));
+  ZKB_TRY(check_align(b, 16, "b"));
+  ZKB_TRY(check_align(out, 16, "out"));
   k_g1_add_affine<<<grid_for(n, 128), 128, 0, as_stream(stream)>>>(a, a_step, b, b_step, out, n);
   return check_launch("g1_add_affine launch");
 }
@@ -165,6 +171,8 @@ int zkb_g1_double(const uint64_t* a, uint64_t* out, int64_t n, void* stream) {
   ZKB_TRY(check_steps(n, 1, 1));
   if (n == 0) return ZKB_OK;
   if (!a || !out) return fail(ZKB_EINVAL, "null buffer");
+  ZKB_TRY(check_align(a, 16, "a"));
+  ZKB_TRY(check_align(out, 16, "out"));
   k_g1_double<<<grid_for(n, 128), 128, 0, as_stream(stream)>>>(a, out, n);
   return check_launch("g1_double launch");
 }
@@ -174,6 +182,8 @@ int zkb_g1_to_affine(const uint64_t* jac, uint64_t* out, int64_t n, void* stream
   ZKB_TRY(check_steps(n, 1, 1));
   if (n == 0) return ZKB_OK;
   if (!jac || !out) return fail(ZKB_EINVAL, "null buffer");
+  ZKB_TRY(check_align(jac, 16, "jac"));
+  ZKB_TRY(check_align(out, 16, "out"));
   k_g1_to_affine<<<grid_for(n, 128), 128, 0, as_stream(stream)>>>(jac, out, n);
   return check_launch("g1_to_affine launch");
 }
@@ -183,6 +193,8 @@ int zkb_g1_mul_generator(const uint64_t* k, uint64_t* out, int64_t n, void* stre
   ZKB_TRY(check_steps(n, 1, 1));
   if (n == 0) return ZKB_OK;
   if (!k || !out) return fail(ZKB_EINVAL, "null buffer");
+  ZKB_TRY(check_align(k, 16, "k"));
+  ZKB_TRY(check_align(out, 16, "out"));
   k_g1_mul_generator<<<grid_for(n, 128), 128, 0, as_stream(stream)>>>(k, out, n);
   return check_launch("g1_mul_generator launch");
 }
@@ -191,6 +203,8 @@ int zkb_g1_check_affine(const uint64_t* points, int64_t n, int64_t* first_bad, v
   set_error("%s", "");
   ZKB_TRY(check_steps(n, 1, 1));
   if (!first_bad) return fail(ZKB_EINVAL, "null result pointer");
+  ZKB_TRY(check_align(first_bad, 8, "first_bad"));
+  ZKB_TRY(check_align(points, 16, "points"));
   cudaStream_t s = as_stream(stream);
   unsigned long long* fb = reinterpret_cast<unsigned long long*>(first_bad);
   // all ones reads back as -1 when no point fails

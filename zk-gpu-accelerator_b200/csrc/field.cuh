@@ -354,10 +354,14 @@ __device__ __noinline__ void fe_pow(uint32_t r[8], const uint32_t a[8], const ui
 template <class F>
 __device__ __forceinline__ void fe_inv(uint32_t r[8], const uint32_t a[8], const F& f) {
   uint32_t e[8];
-  // p - 2: p is odd, so only the low limb changes (p >= 3, no borrow).
+  // e = p - 2, borrowing through the limbs (a low limb of 0 or 1 borrows)
+  uint32_t borrow = 2;
 #pragma unroll
-  for (int j = 0; j < 8; ++j) e[j] = f.p(j);
-  e[0] -= 2u;
+  for (int j = 0; j < 8; ++j) {
+    const uint32_t pj = f.p(j);
+    e[j] = pj - borrow;
+    borrow = pj < borrow ? 1u : 0u;
+  }
   fe_pow(r, a, e, f);
 }
 

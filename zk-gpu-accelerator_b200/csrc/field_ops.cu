@@ -69,6 +69,9 @@ static int field_binary(const zkb_field* f, const uint64_t* a, int64_t a_step, c
   }
   if (n == 0) return ZKB_OK;
   if (!a || !b || !out) return fail(ZKB_EINVAL, "null buffer");
+  ZKB_TRY(check_align(a, 16, "a"));
+  ZKB_TRY(check_align(b, 16, "b"));
+  ZKB_TRY(check_align(out, 16, "out"));
   const int threads = 256;
   const unsigned grid = grid_for(n, threads);
   cudaStream_t s = as_stream(stream);
@@ -106,6 +109,8 @@ int zkb_field_to_mont(const zkb_field* f, const uint64_t* in, uint64_t* out, int
   if (n < 0) return fail(ZKB_EINVAL, "negative row count");
   if (n == 0) return ZKB_OK;
   if (!in || !out) return fail(ZKB_EINVAL, "null buffer");
+  ZKB_TRY(check_align(in, 16, "in"));
+  ZKB_TRY(check_align(out, 16, "out"));
   // BN254's moduli exceed 2^253, so five subtractions reduce any 256-bit value.
   const int subs = f->kind == ZKB_FIELD_GENERIC ? 0 : 5;
   const unsigned grid = grid_for(n, 256);
@@ -123,6 +128,8 @@ int zkb_field_from_mont(const zkb_field* f, const uint64_t* in, uint64_t* out, i
   if (n < 0) return fail(ZKB_EINVAL, "negative row count");
   if (n == 0) return ZKB_OK;
   if (!in || !out) return fail(ZKB_EINVAL, "null buffer");
+  ZKB_TRY(check_align(in, 16, "in"));
+  ZKB_TRY(check_align(out, 16, "out"));
   const unsigned grid = grid_for(n, 256);
   cudaStream_t s = as_stream(stream);
   return with_field(f, [&](auto fp) {

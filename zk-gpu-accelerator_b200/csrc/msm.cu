@@ -288,8 +288,12 @@ __global__ void k_msm_finalize(const uint64_t* window_sums, int W, int w, uint64
     fe_from_mont(x, x, f);
     fe_from_mont(y, y, f);
   }
-  fe_store(result, x);
-  fe_store(result + 4, y);
+  // 8-byte stores: the result buffer only has to be 8-byte aligned
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    result[j] = (uint64_t)x[2 * j] | ((uint64_t)x[2 * j + 1] << 32);
+    result[4 + j] = (uint64_t)y[2 * j] | ((uint64_t)y[2 * j + 1] << 32);
+  }
   result[8] = flag;
 }
 
@@ -512,12 +516,16 @@ int zkb_msm(const uint64_t* points, const uint64_t* scalars, int64_t n, int wind
                 kMsmMaxWindow, window_size);
   }
   if (!result) return fail(ZKB_EINVAL, "null result buffer");
+  ZKB_TRY(check_align(result, 8, "result"));
   cudaStream_t s = as_stream(stream);
   if (n == 0) {
     k_msm_identity_result<<<1, 1, 0, s>>>(result);
     return check_launch("msm identity");
   }
   if (!points || !scalars) return fail(ZKB_EINVAL, "null buffer");
+  ZKB_TRY(check_align(points, 16, "points"));
+  ZKB_TRY(check_align(scalars, 16, "scalars"));
+  ZKB_TRY(check_align(workspace, 256, "workspace"));
   const int w = window_size ? window_size : default_window(n);
   MsmPlan p;
   ZKB_TRY(make_plan(n, w, p));

@@ -584,6 +584,9 @@ int zkb_ntt(const zkb_field* f, const uint64_t* in, uint64_t* out, int64_t n, in
   if (n == 0) return ZKB_OK;
   if (!in || !out) return fail(ZKB_EINVAL, "null buffer");
   if (in == out) return fail(ZKB_EINVAL, "NTT output must not alias its input");
+  ZKB_TRY(check_align(in, 16, "in"));
+  ZKB_TRY(check_align(out, 16, "out"));
+  ZKB_TRY(check_align(workspace, 16, "workspace"));
   if (!omega && f->kind != ZKB_FIELD_BN254_FR) {
     return fail(ZKB_EINVAL, "a root of unity is required for fields other than BN254 Fr");
   }
