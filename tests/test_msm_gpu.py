@@ -94,7 +94,8 @@ def test_bucket_edge_cases():
 def test_reduces_scalars_mod_r():
     three = po.scalar_mul(po.G, 3)
     for scalar in (-5, R, R + 7, 2**300 + 1):
-        assert msm_pippenger_gpu([three[0]], [three[1]], [scalar]) == Point(*po.scalar_mul(three, scalar % R))
+        want = po.scalar_mul(three, scalar % R)
+        assert msm_pippenger_gpu([three[0]], [three[1]], [scalar]) == (Point.identity() if want is None else Point(*want))
 
 
 def test_returns_a_point():
