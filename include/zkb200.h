@@ -162,6 +162,25 @@ size_t zkb_msm_workspace_bytes(int64_t n, int window_size);
 int zkb_msm(const uint64_t* points, const uint64_t* scalars, int64_t n, int window_size,
             uint64_t* result, void* workspace, size_t workspace_bytes, void* stream);
 
+/* MSM for callers that cannot allocate device memory at call time: a plugin
+ * living inside a framework that owns all device memory through its own
+ * allocator, or a serving loop that must never reach cudaMalloc because it
+ * can synchronise the whole device. It has no counterpart in the reference.
+ * Same inputs, result and result layout as zkb_msm, but no workspace: the
+ * scratch is a fixed 64 MiB array inside the library (zkb_msm_no_alloc_capacity()),
+ * which every GPU that loads the library keeps until the process exits. That
+ * covers 2^16 points at the default window; a problem that needs more returns
+ * ZKB_EWORKSPACE. The first call on each device looks up the array's device
+ * address (with that device current); make that first call before any stream
+ * capture. All calls share the array, so calls whose work overlaps on the GPU
+ * (other streams or other host threads) race: order them, e.g. on one stream.
+ * Nothing is allocated or freed. */
+int zkb_msm_no_alloc(const uint64_t* points, const uint64_t* scalars, int64_t n, int window_size,
+                     uint64_t* result, void* stream);
+
+/* Size in bytes of the fixed scratch array zkb_msm_no_alloc works in. */
+size_t zkb_msm_no_alloc_capacity(void);
+
 /* ---- measurement -------------------------------------------------------- */
 
 /* Number of this library's own kernels launched so far in this process

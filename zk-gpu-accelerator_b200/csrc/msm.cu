@@ -29,6 +29,7 @@
 // and the last term is the same problem on the L S_t with delta = 0.
 #include <cub/device/device_radix_sort.cuh>
 
+#include <mutex>
 #include <vector>
 
 #include "curve.cuh"
@@ -538,6 +539,95 @@ int zkb_msm(const uint64_t* points, const uint64_t* scalars, int64_t n, int wind
                 (long long)n, w, p.total, workspace_bytes);
   }
   return run_msm(points, scalars, p, result, reinterpret_cast<char*>(workspace), s);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// MSM without any allocation: scratch in a fixed device array
+// ---------------------------------------------------------------------------
+//
+// zkb_msm takes its scratch memory from the caller. Some callers have no way
+// to hand over device memory at call time: a plugin running inside another
+// framework whose device memory is all reserved up front by that framework's
+// own allocator, or a latency-critical serving loop that must never reach
+// cudaMalloc (which can synchronise the whole device and stall every other
+// stream). zkb_msm_no_alloc serves them: it runs the very same MSM pipeline on
+// a scratch array that is part of the library itself.
+//
+// The array below is a file-scope device variable: every GPU on which the
+// library is loaded holds these 64 MiB until the process exits, whether or
+// not the entry point is ever called. That is enough scratch for 2^16 points
+// at the default window; larger problems are refused with ZKB_EWORKSPACE.
+// All calls share the one array per device, so two calls whose work overlaps
+// on the GPU (different streams, or different host threads) corrupt each
+// other's results: callers must order them, for example on one stream.
+// Every buffer the pipeline reads is fully rewritten by the call itself (the
+// buckets are reset to the identity, every key and slot is written before it
+// is read), so a call never depends on what the previous one left behind.
+
+namespace zkb {
+
+static constexpr size_t kNoAllocScratchBytes = 64ull << 20;
+static __device__ __align__(256) unsigned char g_msm_static_scratch[kNoAllocScratchBytes];
+
+// Device address of g_msm_static_scratch per device, looked up once per device
+// (with that device current) on the first call there.
+static std::mutex g_static_scratch_mutex;
+static void* g_static_scratch_addr[64] = {};
+
+static int static_scratch_address(void** out) {
+  int dev = 0;
+  ZKB_TRY(check_cuda(cudaGetDevice(&dev), "cudaGetDevice"));
+  if (dev < 0 || dev >= 64) return fail(ZKB_EINVAL, "device index %d out of range", dev);
+  std::lock_guard<std::mutex> lock(g_static_scratch_mutex);
+  if (!g_static_scratch_addr[dev]) {
+    void* ptr = nullptr;
+    ZKB_TRY(check_cuda(cudaGetSymbolAddress(&ptr, g_msm_static_scratch),
+                       "cudaGetSymbolAddress(static MSM scratch)"));
+    g_static_scratch_addr[dev] = ptr;
+  }
+  *out = g_static_scratch_addr[dev];
+  return ZKB_OK;
+}
+
+}  // namespace zkb
+
+extern "C" {
+
+size_t zkb_msm_no_alloc_capacity(void) { return zkb::kNoAllocScratchBytes; }
+
+int zkb_msm_no_alloc(const uint64_t* points, const uint64_t* scalars, int64_t n, int window_size,
+                     uint64_t* result, void* stream) {
+  set_error("%s", "");
+  if (n < 0) return fail(ZKB_EINVAL, "negative point count");
+  if (n >= (1ll << 31)) return fail(ZKB_EINVAL, "at most 2^31 - 1 points per MSM");
+  if (window_size < 0 || window_size > kMsmMaxWindow) {
+    return fail(ZKB_EINVAL, "window_size must be in 1..%d (or 0 for the default), got %d",
+                kMsmMaxWindow, window_size);
+  }
+  if (!result) return fail(ZKB_EINVAL, "null result buffer");
+  ZKB_TRY(check_align(result, 8, "result"));
+  cudaStream_t s = as_stream(stream);
+  if (n == 0) {
+    k_msm_identity_result<<<1, 1, 0, s>>>(result);
+    return check_launch("msm identity");
+  }
+  if (!points || !scalars) return fail(ZKB_EINVAL, "null buffer");
+  ZKB_TRY(check_align(points, 16, "points"));
+  ZKB_TRY(check_align(scalars, 16, "scalars"));
+  const int w = window_size ? window_size : default_window(n);
+  MsmPlan p;
+  ZKB_TRY(make_plan(n, w, p));
+  if (p.total > kNoAllocScratchBytes) {
+    return fail(ZKB_EWORKSPACE,
+                "MSM of %lld points at window %d needs %zu bytes of scratch; the library's fixed "
+                "scratch holds %zu bytes (use zkb_msm with a caller-provided workspace)",
+                (long long)n, w, p.total, kNoAllocScratchBytes);
+  }
+  void* scratch = nullptr;
+  ZKB_TRY(static_scratch_address(&scratch));
+  return run_msm(points, scalars, p, result, reinterpret_cast<char*>(scratch), s);
 }
 
 }  // extern "C"

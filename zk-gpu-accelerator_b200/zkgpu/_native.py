@@ -77,6 +77,8 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "zkb_msm_default_window": (ctypes.c_int, [_i64]),
     "zkb_msm_workspace_bytes": (ctypes.c_size_t, [_i64, ctypes.c_int]),
     "zkb_msm": (ctypes.c_int, [_u64p, _u64p, _i64, ctypes.c_int, _u64p, _vp, ctypes.c_size_t, _vp]),
+    "zkb_msm_no_alloc": (ctypes.c_int, [_u64p, _u64p, _i64, ctypes.c_int, _u64p, _vp]),
+    "zkb_msm_no_alloc_capacity": (ctypes.c_size_t, []),
     "zkb_launch_count": (ctypes.c_uint64, []),
     "zkb_profile_enable": (None, [ctypes.c_int]),
     "zkb_profile_report": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_size_t]),
