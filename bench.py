@@ -338,7 +338,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     achieved = imad / (acc_avg_ms * 1e-3) / 1e12
     acc_bytes = madds * (64 + 8) + 2 * (-(-madds // 64)) * 132  # point gathers + sorted pairs + partial slots
     hbm_peak = peaks.get("hbm_gbs")
-    traffic = _profile_traffic("msm_acc_points", step.n)
+    traffic = _profile_traffic("k_msm_acc_points", step.n)
     roofline = {
         "kernel": "k_msm_acc_points (bucket accumulation, uniform scalars)",
         "bound": "imad",
