@@ -73,35 +73,45 @@ IMAD_PER_MULMOD = 264  # 2 x 64 32-bit multiply-adds (lo and hi) for a*b and m*p
 MULMOD_PER_MADD = 10   # XYZZ mixed addition: 8 multiplications + 2 squarings
 
 
-def nonzero_digits(scalars, w: int) -> int:
-    """Nonzero signed w-bit digits over all windows: the pairs the bucket kernel adds
-    (same recoding as csrc/msm.cu: windows of w bits, digit > 2^(w-1) borrows)."""
+# GLV split constants (csrc/msm.cu): k = k1 + k2 lambda, c1 = floor(k g1 / 2^256), ...
+_R = 21888242871839275222246405745257275088548364400416034343698204186575808495617
+_GLV_A1 = 9931322734385697763
+_GLV_B1_ABS = 147946756881789319000765030803803410728
+_GLV_A2 = 147946756881789319010696353538189108491
+_GLV_G1 = 0x2D91D232EC7E0B3D7
+_GLV_G2 = 0x24CCEF014A773D2CF7A7BD9D4391EB18E
+
+
+def _glv_halves(k: int) -> tuple[int, int]:
+    c1, c2 = (k * _GLV_G1) >> 256, (k * _GLV_G2) >> 256
+    return abs(k - c1 * _GLV_A1 - c2 * _GLV_A2), abs(c1 * _GLV_B1_ABS - c2 * _GLV_A1)
+
+
+def nonzero_digits(scalars, w: int, sample: int = 1 << 16) -> int:
+    """Mixed additions the bucket kernel performs: nonzero signed w-bit digits of
+    both GLV halves (csrc/msm.cu's recoding: ceil(128 / w) windows, a digit above
+    2^(w-1) borrows). Counted exactly on the first `sample` scalars, scaled to n."""
     import numpy as np
 
+    from zkgpu import workloads as wl
+
     n = scalars.shape[0]
-    W = -(-(SCALAR_BITS + 1) // w)
+    m = min(n, sample)
+    W = -(-128 // w)
     half = 1 << (w - 1)
-    carry = np.zeros(n, dtype=np.int64)
-    total = 0
-    limbs = [scalars[:, j].astype(np.uint64) for j in range(4)]
-    for win in range(W):
-        lo = win * w
-        limb, off = lo // 64, lo % 64
-        if limb < 4:
-            v = limbs[limb] >> np.uint64(off)
-            if off + w > 64 and limb + 1 < 4:
-                v = v | (limbs[limb + 1] << np.uint64(64 - off))
-            raw = (v & np.uint64((1 << w) - 1)).astype(np.int64) + carry
-        else:
-            raw = carry.copy()
-        if win + 1 < W:
-            borrow = raw > half
-            mag = np.where(borrow, (1 << w) - raw, raw)
-            carry = borrow.astype(np.int64)
-        else:
-            mag = raw
-        total += int(np.count_nonzero(mag))
-    return total
+    mask = (1 << w) - 1
+    count = 0
+    for k in wl.rows_to_ints(np.ascontiguousarray(scalars[:m])):
+        for v in _glv_halves(k % _R):
+            carry = 0
+            for win in range(W):
+                raw = ((v >> (win * w)) & mask) + carry
+                if win + 1 < W and raw > half:
+                    mag, carry = (1 << w) - raw, 1
+                else:
+                    mag, carry = raw, 0
+                count += mag != 0
+    return round(count * n / m)
 
 
 # ------------------------------------------------------------------

@@ -82,9 +82,10 @@ def test_host_only_queries():
     lib = _native.lib()
     assert lib.zkb_ntt_workspace_bytes(4096) == 0
     assert lib.zkb_ntt_workspace_bytes(1 << 20) == 32 << 20
-    # default window: argmin of windows * (10 n + 42 * 2^(w-1)), signed digits
+    # default window: argmin of windows * (20 n + 42 * 2^(w-1)): signed digits over
+    # the two 127-bit GLV halves, ceil(128 / w) windows
     def model(n):
-        best = min(range(1, 17), key=lambda w: (-(-255 // w)) * (10 * n + 42 * 2 ** (w - 1)))
+        best = min(range(1, 17), key=lambda w: (-(-128 // w)) * (20 * n + 42 * 2 ** (w - 1)))
         return best if n > 1 else 1
     for n in (1, 100, 2**12, 2**16, 2**20, 2**22):
         assert lib.zkb_msm_default_window(n) == model(n), n

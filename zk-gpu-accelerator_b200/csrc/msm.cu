@@ -42,9 +42,163 @@ static constexpr int kMsmMaxWindow = 20;
 static constexpr int kAcc1PerThread = 64;   // K1: sorted pairs per level-1 thread
 static constexpr int kSlotPerThread = 32;   // K2: slots per merge thread
 static constexpr int kReduceLogL = 3;       // reduction segments of 8 entries
-static constexpr int kScalarBits = 254;     // r < 2^254
+static constexpr int kHalfBits = 128;       // GLV halves: |k1|, |k2| < 2^127
 
-static int num_windows(int w) { return (kScalarBits + 1 + w - 1) / w; }
+// Windows per GLV half: signed digits need W w >= 128 so that the top window
+// (at most 127 - (W - 1) w value bits, plus a borrow) never exceeds 2^(w-1).
+static int num_windows(int w) { return (kHalfBits + w - 1) / w; }
+
+// ---------------------------------------------------------------------------
+// GLV: BN254 G1 has the endomorphism phi(x, y) = (beta x, y) = lambda (x, y)
+// for cube roots of unity beta in Fq and lambda in Fr. Each scalar splits as
+// k = k1 + k2 lambda (mod r) with |k1|, |k2| < 2^127, so sum k_i P_i =
+// sum k1_i P_i + k2_i phi(P_i): twice the points at half the bits. The
+// accumulation work is unchanged, but the windows (and so the bucket
+// reduction) halve, and the final doubling chain is 112 doublings instead of
+// 240. Only the affine sum is compared with the reference, which is the same
+// for every decomposition.
+//
+// Decomposition (Babai rounding against the reduced lattice basis
+// v1 = (a1, b1), v2 = (a2, b2) of {(x, y): x + y lambda = 0 mod r}, computed
+// offline from lambda by the extended Euclidean algorithm):
+//   c1 = floor(k g1 / 2^256), g1 = round(b2 2^256 / r)
+//   c2 = floor(k g2 / 2^256), g2 = round(-b1 2^256 / r)
+//   k1 = k - c1 a1 - c2 a2,   k2 = -c1 b1 - c2 b2
+// The exact products cancel (a1 b2 - a2 b1 = r), leaving
+// |k1| <= |a1| + |a2| < 2^127 and |k2| <= |b1| + |b2| < 2^127.
+// ---------------------------------------------------------------------------
+
+// beta (Montgomery form over Fq), the cube root of unity with phi = lambda.
+// beta = 0x59e26bcea0d48bacd4f263f1acdb5c4f5763473177fffffe.
+__device__ __forceinline__ void glv_beta_mont(uint32_t r[8]) {
+  const uint32_t beta[8] = {0x77fffffeu, 0x57634731u, 0xacdb5c4fu, 0xd4f263f1u,
+                            0xa0d48bacu, 0x59e26bceu, 0u, 0u};
+  fe_to_mont(r, beta, FqP{});
+}
+
+// Basis and rounding constants, little-endian 32-bit limbs:
+//   a1 = b2 = 9931322734385697763 (64 bits)
+//   b1 = -147946756881789319000765030803803410728 (|b1| has 127 bits)
+//   a2 = 147946756881789319010696353538189108491 (127 bits)
+//   g1 = round(b2 2^256 / r) (66 bits), g2 = round(-b1 2^256 / r) (130 bits)
+__device__ __forceinline__ uint32_t glv_a1(int i) {
+  constexpr uint32_t v[2] = {0x94d213e3u, 0x89d32568u};
+  return v[i];
+}
+__device__ __forceinline__ uint32_t glv_b1_abs(int i) {
+  constexpr uint32_t v[4] = {0x7d4f1128u, 0x8211bbebu, 0xeeb859fcu, 0x6f4d8248u};
+  return v[i];
+}
+__device__ __forceinline__ uint32_t glv_a2(int i) {
+  constexpr uint32_t v[4] = {0x1221250bu, 0x0be4e154u, 0xeeb859fdu, 0x6f4d8248u};
+  return v[i];
+}
+__device__ __forceinline__ uint32_t glv_g1(int i) {
+  constexpr uint32_t v[3] = {0xc7e0b3d7u, 0xd91d232eu, 0x00000002u};
+  return v[i];
+}
+__device__ __forceinline__ uint32_t glv_g2(int i) {
+  constexpr uint32_t v[5] = {0x391eb18eu, 0x7a7bd9d4u, 0xa773d2cfu, 0x4ccef014u, 0x00000002u};
+  return v[i];
+}
+
+// k1, k2 (as 128-bit magnitudes with signs) for a scalar k < r (8 limbs).
+__device__ __forceinline__ void glv_split(const uint32_t k[8], uint32_t k1[4], uint32_t& neg1,
+                                          uint32_t k2[4], uint32_t& neg2) {
+  // c1 = floor(k g1 / 2^256): limbs 8..9 of the 8 x 3 product
+  uint32_t p1[11];
+#pragma unroll
+  for (int i = 0; i < 11; ++i) p1[i] = 0;
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    uint64_t c = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const uint64_t t = (uint64_t)k[i] * glv_g1(j) + p1[i + j] + c;
+      p1[i + j] = (uint32_t)t;
+      c = t >> 32;
+    }
+    p1[8 + j] = (uint32_t)c;
+  }
+  const uint32_t c1[2] = {p1[8], p1[9]};
+  // c2 = floor(k g2 / 2^256): limbs 8..11 of the 8 x 5 product
+  uint32_t p2[13];
+#pragma unroll
+  for (int i = 0; i < 13; ++i) p2[i] = 0;
+#pragma unroll
+  for (int j = 0; j < 5; ++j) {
+    uint64_t c = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const uint64_t t = (uint64_t)k[i] * glv_g2(j) + p2[i + j] + c;
+      p2[i + j] = (uint32_t)t;
+      c = t >> 32;
+    }
+    p2[8 + j] = (uint32_t)c;
+  }
+  const uint32_t c2[4] = {p2[8], p2[9], p2[10], p2[11]};
+  // low 128 bits of c1 a1, c2 a2, c1 |b1|, c2 b2
+  uint32_t t1[4] = {0, 0, 0, 0}, t2[4] = {0, 0, 0, 0}, t3[4] = {0, 0, 0, 0}, t4[4] = {0, 0, 0, 0};
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    uint64_t ca = 0, cb = 0;
+#pragma unroll
+    for (int j = 0; i + j < 4; ++j) {
+      const uint64_t x = (uint64_t)c1[i] * (j < 2 ? glv_a1(j) : 0u) + t1[i + j] + ca;
+      t1[i + j] = (uint32_t)x;
+      ca = x >> 32;
+      const uint64_t y = (uint64_t)c1[i] * glv_b1_abs(j) + t3[i + j] + cb;
+      t3[i + j] = (uint32_t)y;
+      cb = y >> 32;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    uint64_t ca = 0, cb = 0;
+#pragma unroll
+    for (int j = 0; i + j < 4; ++j) {
+      const uint64_t x = (uint64_t)c2[i] * glv_a2(j) + t2[i + j] + ca;
+      t2[i + j] = (uint32_t)x;
+      ca = x >> 32;
+      const uint64_t y = (uint64_t)c2[i] * (j < 2 ? glv_a1(j) : 0u) + t4[i + j] + cb;  // b2 = a1
+      t4[i + j] = (uint32_t)y;
+      cb = y >> 32;
+    }
+  }
+  // k1 = k - t1 - t2 and k2 = t3 - t4, both mod 2^128 (the true values lie in
+  // (-2^127, 2^127)); the carry is signed: floor(d / 2^32) by arithmetic shift
+  int64_t carry = 0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int64_t d = (int64_t)k[i] - (int64_t)t1[i] - (int64_t)t2[i] + carry;
+    k1[i] = (uint32_t)d;
+    carry = d >> 32;
+  }
+  carry = 0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int64_t d = (int64_t)t3[i] - (int64_t)t4[i] + carry;
+    k2[i] = (uint32_t)d;
+    carry = d >> 32;
+  }
+  // magnitudes and signs
+  neg1 = k1[3] >> 31;
+  neg2 = k2[3] >> 31;
+  uint64_t c = 1;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const uint64_t v = (uint64_t)(neg1 ? ~k1[i] : k1[i]) + (neg1 ? c : 0);
+    k1[i] = (uint32_t)v;
+    c = v >> 32;
+  }
+  c = 1;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const uint64_t v = (uint64_t)(neg2 ? ~k2[i] : k2[i]) + (neg2 ? c : 0);
+    k2[i] = (uint32_t)v;
+    c = v >> 32;
+  }
+}
 
 // ---------------------------------------------------------------------------
 // 1. digits
@@ -52,46 +206,77 @@ static int num_windows(int w) { return (kScalarBits + 1 + w - 1) / w; }
 
 // Bits [lo, lo + w) of a 256-bit little-endian value (w <= 20 spans two limbs
 // at most).
-__device__ __forceinline__ uint32_t scalar_bits(const uint32_t s[8], int lo, int w) {
+// Bits [lo, lo + w) of a 128-bit little-endian magnitude (w <= 20, so at most
+// two limbs; bits at and above 128 are zero).
+__device__ __forceinline__ uint32_t half_bits(const uint32_t s[4], int lo, int w) {
+  if (lo >= 128) return 0;
   const int limb = lo >> 5, off = lo & 31;
   uint64_t v = s[limb];
-  if (limb + 1 < 8) v |= (uint64_t)s[limb + 1] << 32;
+  if (limb + 1 < 4) v |= (uint64_t)s[limb + 1] << 32;
   return (uint32_t)(v >> off) & ((1u << w) - 1u);
 }
 
+// Signed w-bit digits of one GLV half |k| (sign neg) of point `point`: the pair
+// (key, value) for window win goes to entry (half * W + win) * n + i.
+__device__ __forceinline__ void emit_digits(const uint32_t k[4], uint32_t neg, uint32_t point,
+                                            int64_t first_entry, int64_t n, int w, int W,
+                                            uint32_t none, uint32_t* keys, uint32_t* vals) {
+  const uint32_t half = 1u << (w - 1);
+  uint32_t carry = 0;
+  for (int win = 0; win < W; ++win) {
+    const uint32_t raw = half_bits(k, win * w, w) + carry;
+    uint32_t mag, dneg = 0;
+    if (win + 1 < W && raw > half) {
+      // raw - 2^w in [-(2^(w-1) - 1), 0], borrowing 1 from the next window
+      mag = (1u << w) - raw;
+      dneg = 1;
+      carry = 1;
+    } else {
+      mag = raw;
+      carry = 0;
+    }
+    const int64_t e = first_entry + (int64_t)win * n;
+    if (mag == 0) {
+      keys[e] = none;
+      vals[e] = 0;
+    } else {
+      keys[e] = ((uint32_t)win << (w - 1)) | (mag - 1);
+      vals[e] = point | ((neg ^ dneg) << 31);
+    }
+  }
+}
+
+// One thread per scalar: reduce mod r, split k = k1 + k2 lambda, and emit the
+// digits of k1 (points 0..n-1) and of k2 (points n..2n-1, the phi images).
 __global__ void __launch_bounds__(256) k_msm_digits(const uint64_t* scalars, int64_t n, int w,
                                                     int W, uint32_t none, uint32_t* keys,
                                                     uint32_t* vals) {
   FrP fr;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  const uint32_t half = 1u << (w - 1);
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
     uint32_t s[8];
     fe_load_nc(s, scalars + 4 * i);
     fe_reduce_full(s, fr, 5);  // any 256-bit value -> [0, r)
-    uint32_t carry = 0;
-    for (int win = 0; win < W; ++win) {
-      const int lo = win * w;
-      uint32_t raw = (lo < 256 ? scalar_bits(s, lo, w > 256 - lo ? 256 - lo : w) : 0) + carry;
-      uint32_t mag, neg = 0;
-      if (win + 1 < W && raw > half) {
-        // raw - 2^w in [-(2^(w-1) - 1), -1], borrow 1 from the next window
-        mag = (1u << w) - raw;
-        neg = 1;
-        carry = 1;
-      } else {
-        mag = raw;
-        carry = 0;
-      }
-      const int64_t e = (int64_t)win * n + i;
-      if (mag == 0) {
-        keys[e] = none;
-        vals[e] = 0;
-      } else {
-        keys[e] = ((uint32_t)win << (w - 1)) | (mag - 1);
-        vals[e] = (uint32_t)i | (neg << 31);
-      }
-    }
+    uint32_t k1[4], k2[4], neg1, neg2;
+    glv_split(s, k1, neg1, k2, neg2);
+    emit_digits(k1, neg1, (uint32_t)i, i, n, w, W, none, keys, vals);
+    emit_digits(k2, neg2, (uint32_t)(n + i), (int64_t)W * n + i, n, w, W, none, keys, vals);
+  }
+}
+
+// phi(P_i) = (beta x_i, y_i), the points that the k2 halves multiply.
+__global__ void __launch_bounds__(256) k_msm_phi(const uint64_t* points, int64_t n, uint64_t* phi) {
+  FqP f;
+  uint32_t beta[8];
+  glv_beta_mont(beta);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    uint32_t x[8], y[8];
+    fe_load_nc(x, points + 8 * i);
+    fe_load_nc(y, points + 8 * i + 4);
+    fe_mul(x, x, beta, f);
+    fe_store(phi + 8 * i, x);
+    fe_store(phi + 8 * i + 4, y);
   }
 }
 
@@ -149,6 +334,7 @@ struct RunSink {
 // Level 1: K1 sorted (key, value) pairs per thread, mixed additions of affine
 // input points.
 __global__ void __launch_bounds__(128) k_msm_acc_points(const uint64_t* points,
+                                                        const uint64_t* phi, int64_t n,
                                                         const uint32_t* keys,
                                                         const uint32_t* vals, int64_t E, int K,
                                                         uint32_t none, uint64_t* buckets,
@@ -176,8 +362,9 @@ __global__ void __launch_bounds__(128) k_msm_acc_points(const uint64_t* points,
     }
     if (k == none) break;  // zero digits sort last: nothing after them
     const uint32_t v = vals[e];
+    const int64_t idx = (int64_t)(v & 0x7fffffffu);
     Aff q;
-    aff_load_nc(q, points + 8 * (int64_t)(v & 0x7fffffffu));
+    aff_load_nc(q, idx < n ? points + 8 * idx : phi + 8 * (idx - n));
     if (v >> 31) aff_neg(q);
     xyzz_add_affine(acc, q);
   }
@@ -308,14 +495,16 @@ __global__ void k_msm_identity_result(uint64_t* result) {
 // ---------------------------------------------------------------------------
 
 int default_window(int64_t n) {
-  // argmin over w of windows * (cost of n mixed additions + 2^(w-1) buckets'
-  // share of the reduction), in units of field multiplications: 10 per mixed
-  // addition, about 42 per bucket in the running sums.
+  // argmin over w of windows * (cost of the 2n GLV-half mixed additions +
+  // 2^(w-1) buckets' share of the reduction), in units of field
+  // multiplications: 10 per mixed addition, about 42 per bucket in the
+  // running sums.
   if (n <= 1) return 1;
   int best_w = 1;
   double best = 1e300;
   for (int w = 1; w <= 16; ++w) {
-    const double cost = (double)num_windows(w) * (10.0 * (double)n + 42.0 * (double)(1ll << (w - 1)));
+    const double cost =
+        (double)num_windows(w) * (20.0 * (double)n + 42.0 * (double)(1ll << (w - 1)));
     if (cost < best) {
       best = cost;
       best_w = w;
@@ -336,9 +525,9 @@ struct MsmPlan {
   std::vector<int64_t> slot_levels;  // thread count of each merge level
   size_t cub_bytes = 0;
   // workspace offsets
-  size_t off_keys0, off_keys1, off_vals0, off_vals1, off_cub, off_buckets, off_slot_keys_a,
-      off_slot_pts_a, off_slot_keys_b, off_slot_pts_b, off_red_s0, off_red_u0, off_red_s1,
-      off_red_u1, off_wsum, total;
+  size_t off_keys0, off_keys1, off_vals0, off_vals1, off_cub, off_phi, off_buckets,
+      off_slot_keys_a, off_slot_pts_a, off_slot_keys_b, off_slot_pts_b, off_red_s0, off_red_u0,
+      off_red_s1, off_red_u1, off_wsum, total;
 };
 
 static int make_plan(int64_t n, int w, MsmPlan& p) {
@@ -351,7 +540,7 @@ static int make_plan(int64_t n, int w, MsmPlan& p) {
   while ((1ll << bits) <= keys_used) ++bits;  // keys_used itself must fit below none
   p.key_bits = bits;
   p.none = (uint32_t)((1ull << bits) - 1);
-  p.E = (int64_t)p.W * n;
+  p.E = 2 * (int64_t)p.W * n;  // both GLV halves
   p.T1 = (p.E + kAcc1PerThread - 1) / kAcc1PerThread;
   p.slot_levels.clear();
   int64_t M = 2 * p.T1;
@@ -380,6 +569,7 @@ static int make_plan(int64_t n, int w, MsmPlan& p) {
   p.off_vals0 = take((size_t)p.E * 4);
   p.off_vals1 = take((size_t)p.E * 4);
   p.off_cub = take(p.cub_bytes);
+  p.off_phi = take((size_t)n * 64);
   p.off_buckets = take((size_t)p.W * p.nb * 128);
   p.off_slot_keys_a = take((size_t)2 * p.T1 * 4);
   p.off_slot_pts_a = take((size_t)2 * p.T1 * 128);
@@ -404,11 +594,15 @@ static int run_msm(const uint64_t* points, const uint64_t* scalars, const MsmPla
   uint32_t* vals1 = reinterpret_cast<uint32_t*>(ws + p.off_vals1);
   uint64_t* buckets = reinterpret_cast<uint64_t*>(ws + p.off_buckets);
 
-  // 1. digits
+  uint64_t* phi = reinterpret_cast<uint64_t*>(ws + p.off_phi);
+
+  // 1. digits (GLV halves) and the phi images of the points
   {
     ProfSpan span("msm_digits", s);
     k_msm_digits<<<grid_for(p.n, 256), 256, 0, s>>>(scalars, p.n, p.w, p.W, p.none, keys0, vals0);
     ZKB_TRY(check_launch("msm digits"));
+    k_msm_phi<<<grid_for(p.n, 256), 256, 0, s>>>(points, p.n, phi);
+    ZKB_TRY(check_launch("msm phi points"));
   }
 
   // 2. sort
@@ -434,8 +628,8 @@ static int run_msm(const uint64_t* points, const uint64_t* scalars, const MsmPla
   {
     ProfSpan span("msm_acc_points", s);
     const unsigned grid = (unsigned)((p.T1 + 127) / 128);
-    k_msm_acc_points<<<grid, 128, 0, s>>>(points, skeys, svals, p.E, kAcc1PerThread, p.none,
-                                          buckets, sk[0], sp[0]);
+    k_msm_acc_points<<<grid, 128, 0, s>>>(points, phi, p.n, skeys, svals, p.E, kAcc1PerThread,
+                                          p.none, buckets, sk[0], sp[0]);
     ZKB_TRY(check_launch("msm bucket accumulation"));
   }
   {
@@ -511,7 +705,7 @@ int zkb_msm(const uint64_t* points, const uint64_t* scalars, int64_t n, int wind
             uint64_t* result, void* workspace, size_t workspace_bytes, void* stream) {
   set_error("%s", "");
   if (n < 0) return fail(ZKB_EINVAL, "negative point count");
-  if (n >= (1ll << 31)) return fail(ZKB_EINVAL, "at most 2^31 - 1 points per MSM");
+  if (n >= (1ll << 30)) return fail(ZKB_EINVAL, "at most 2^30 - 1 points per MSM");
   if (window_size < 0 || window_size > kMsmMaxWindow) {
     return fail(ZKB_EINVAL, "window_size must be in 1..%d (or 0 for the default), got %d",
                 kMsmMaxWindow, window_size);
@@ -601,7 +795,7 @@ int zkb_msm_no_alloc(const uint64_t* points, const uint64_t* scalars, int64_t n,
                      uint64_t* result, void* stream) {
   set_error("%s", "");
   if (n < 0) return fail(ZKB_EINVAL, "negative point count");
-  if (n >= (1ll << 31)) return fail(ZKB_EINVAL, "at most 2^31 - 1 points per MSM");
+  if (n >= (1ll << 30)) return fail(ZKB_EINVAL, "at most 2^30 - 1 points per MSM");
   if (window_size < 0 || window_size > kMsmMaxWindow) {
     return fail(ZKB_EINVAL, "window_size must be in 1..%d (or 0 for the default), got %d",
                 kMsmMaxWindow, window_size);
