@@ -52,6 +52,7 @@ WORKLOADS = {
     # name: (log2 MSM points, log2 NTT size)
     "large": (22, 24),
     "small": (18, 20),  # for profiler captures: a few GB on the device
+    "tiny": (10, 10),   # for the CPU tests of the reference arm
 }
 
 

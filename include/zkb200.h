@@ -183,6 +183,13 @@ size_t zkb_msm_no_alloc_capacity(void);
 
 /* ---- measurement -------------------------------------------------------- */
 
+/* Tuning knobs, read by each call when it plans its work (so they also change
+ * the workspace size queries): "msm.pairs_per_thread" (default 64),
+ * "msm.slots_per_thread" (8), "msm.reduce_log_segment" (2). ZKB_EINVAL for
+ * an unknown name or a value out of range. Process-wide, not per stream. */
+int zkb_tune_set(const char* key, int value);
+int zkb_tune_get(const char* key, int* value);
+
 /* Number of this library's own kernels launched so far in this process
  * (sorting kernels of the CUB library are not counted). */
 uint64_t zkb_launch_count(void);

@@ -37,6 +37,9 @@ inline int check_cuda(cudaError_t err, const char* what) {
 // Counts this library's own kernel launches (one call per launch).
 void count_launch();
 
+// Tuning knobs read when a call plans its work (zkb_tune_set / zkb_tune_get).
+int tune_get(const char* key);
+
 inline int check_launch(const char* what) {
   count_launch();
   return check_cuda(cudaGetLastError(), what);

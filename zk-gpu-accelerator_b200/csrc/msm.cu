@@ -39,9 +39,6 @@
 namespace zkb {
 
 static constexpr int kMsmMaxWindow = 20;
-static constexpr int kAcc1PerThread = 64;   // K1: sorted pairs per level-1 thread
-static constexpr int kSlotPerThread = 32;   // K2: slots per merge thread
-static constexpr int kReduceLogL = 3;       // reduction segments of 8 entries
 static constexpr int kHalfBits = 128;       // GLV halves: |k1|, |k2| < 2^127
 
 // Windows per GLV half: signed digits need W w >= 128 so that the top window
@@ -520,6 +517,9 @@ struct MsmPlan {
   int w = 0, W = 0, key_bits = 0;
   uint32_t none = 0;
   int64_t nb = 0;  // buckets per window
+  int k1 = 64;     // sorted pairs per bucket thread ("msm.pairs_per_thread")
+  int k2 = 8;      // slots per merge thread ("msm.slots_per_thread")
+  int log_l = 2;   // log2 running-sum segment ("msm.reduce_log_segment")
   int64_t E = 0;   // sorted pairs
   int64_t T1 = 0;  // level-1 threads
   std::vector<int64_t> slot_levels;  // thread count of each merge level
@@ -541,12 +541,15 @@ static int make_plan(int64_t n, int w, MsmPlan& p) {
   p.key_bits = bits;
   p.none = (uint32_t)((1ull << bits) - 1);
   p.E = 2 * (int64_t)p.W * n;  // both GLV halves
-  p.T1 = (p.E + kAcc1PerThread - 1) / kAcc1PerThread;
+  p.k1 = tune_get("msm.pairs_per_thread");
+  p.k2 = tune_get("msm.slots_per_thread");
+  p.log_l = tune_get("msm.reduce_log_segment");
+  p.T1 = (p.E + p.k1 - 1) / p.k1;
   p.slot_levels.clear();
   int64_t M = 2 * p.T1;
   int64_t T = p.T1;
   while (T > 1) {
-    T = (M + kSlotPerThread - 1) / kSlotPerThread;
+    T = (M + p.k2 - 1) / p.k2;
     p.slot_levels.push_back(T);
     M = 2 * T;
   }
@@ -576,7 +579,7 @@ static int make_plan(int64_t n, int w, MsmPlan& p) {
   const int64_t second = p.slot_levels.empty() ? 1 : p.slot_levels[0];
   p.off_slot_keys_b = take((size_t)2 * second * 4);
   p.off_slot_pts_b = take((size_t)2 * second * 128);
-  const int64_t red = (int64_t)p.W * (p.nb >> kReduceLogL > 0 ? p.nb >> kReduceLogL : 1);
+  const int64_t red = (int64_t)p.W * (p.nb >> p.log_l > 0 ? p.nb >> p.log_l : 1);
   p.off_red_s0 = take((size_t)red * 128);
   p.off_red_u0 = take((size_t)red * 128);
   p.off_red_s1 = take((size_t)red * 128);
@@ -628,7 +631,7 @@ static int run_msm(const uint64_t* points, const uint64_t* scalars, const MsmPla
   {
     ProfSpan span("msm_acc_points", s);
     const unsigned grid = (unsigned)((p.T1 + 127) / 128);
-    k_msm_acc_points<<<grid, 128, 0, s>>>(points, phi, p.n, skeys, svals, p.E, kAcc1PerThread,
+    k_msm_acc_points<<<grid, 128, 0, s>>>(points, phi, p.n, skeys, svals, p.E, p.k1,
                                           p.none, buckets, sk[0], sp[0]);
     ZKB_TRY(check_launch("msm bucket accumulation"));
   }
@@ -639,7 +642,7 @@ static int run_msm(const uint64_t* points, const uint64_t* scalars, const MsmPla
     for (size_t lvl = 0; lvl < p.slot_levels.size(); ++lvl) {
       const int64_t T = p.slot_levels[lvl];
       const unsigned grid = (unsigned)((T + 127) / 128);
-      k_msm_acc_slots<<<grid, 128, 0, s>>>(sk[cur], sp[cur], M, kSlotPerThread, p.none, buckets,
+      k_msm_acc_slots<<<grid, 128, 0, s>>>(sk[cur], sp[cur], M, p.k2, p.none, buckets,
                                            sk[cur ^ 1], sp[cur ^ 1]);
       ZKB_TRY(check_launch("msm bucket merge"));
       cur ^= 1;
@@ -659,11 +662,11 @@ static int run_msm(const uint64_t* points, const uint64_t* scalars, const MsmPla
     const uint64_t* U = nullptr;
     int64_t G = p.nb;
     int delta = 1, r = 0;
-    const int64_t L = 1ll << kReduceLogL;
+    const int64_t L = 1ll << p.log_l;
     while (G > L) {
       const int64_t G_out = G / L;
       const int64_t threads = (int64_t)p.W * G_out;
-      k_msm_reduce<<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(X, U, G, kReduceLogL, delta,
+      k_msm_reduce<<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(X, U, G, p.log_l, delta,
                                                                      p.W, rs[r], ru[r], 0);
       ZKB_TRY(check_launch("msm window reduction"));
       X = rs[r];
@@ -672,7 +675,7 @@ static int run_msm(const uint64_t* points, const uint64_t* scalars, const MsmPla
       G = G_out;
       delta = 0;
     }
-    k_msm_reduce<<<(unsigned)((p.W + 127) / 128), 128, 0, s>>>(X, U, G, kReduceLogL, delta, p.W,
+    k_msm_reduce<<<(unsigned)((p.W + 127) / 128), 128, 0, s>>>(X, U, G, p.log_l, delta, p.W,
                                                                nullptr, wsum, 1);
     ZKB_TRY(check_launch("msm window sums"));
   }

@@ -1,6 +1,7 @@
 // runtime.cu — error reporting, version, and the host side of field set-up.
 #include <atomic>
 #include <cstring>
+#include <mutex>
 
 #include "common.cuh"
 #include "field_host.h"
@@ -11,6 +12,33 @@ static thread_local char g_last_error[1024] = "";
 static std::atomic<unsigned long long> g_launches{0};
 
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+// ---- tuning knobs -----------------------------------------------------------
+// name, default, min, max. Read by the planners at each call, so a change
+// applies to the next call (and to the workspace size queries).
+struct Knob {
+  const char* name;
+  int value, lo, hi;
+};
+static Knob g_knobs[] = {
+    {"msm.pairs_per_thread", 64, 8, 4096},   // sorted pairs each bucket thread adds
+    {"msm.slots_per_thread", 8, 4, 4096},    // partial sums each merge thread adds
+    {"msm.reduce_log_segment", 2, 1, 8},     // log2 of the running-sum segment length
+};
+static std::mutex g_knob_mutex;
+
+static Knob* find_knob(const char* key) {
+  if (!key) return nullptr;
+  for (auto& k : g_knobs)
+    if (std::strcmp(k.name, key) == 0) return &k;
+  return nullptr;
+}
+
+int tune_get(const char* key) {
+  std::lock_guard<std::mutex> lock(g_knob_mutex);
+  Knob* k = find_knob(key);
+  return k ? k->value : 0;
+}
 
 void set_error(const char* fmt, ...) {
   va_list ap;
@@ -115,6 +143,27 @@ const char* zkb_last_error(void) { return zkb::g_last_error; }
 int zkb_version(void) { return 100; }
 
 uint64_t zkb_launch_count(void) { return zkb::g_launches.load(); }
+
+int zkb_tune_set(const char* key, int value) {
+  zkb::set_error("%s", "");
+  std::lock_guard<std::mutex> lock(zkb::g_knob_mutex);
+  zkb::Knob* k = zkb::find_knob(key);
+  if (!k) return zkb::fail(ZKB_EINVAL, "unknown tuning knob '%s'", key ? key : "(null)");
+  if (value < k->lo || value > k->hi) {
+    return zkb::fail(ZKB_EINVAL, "%s must be in %d..%d, got %d", k->name, k->lo, k->hi, value);
+  }
+  k->value = value;
+  return ZKB_OK;
+}
+
+int zkb_tune_get(const char* key, int* value) {
+  zkb::set_error("%s", "");
+  std::lock_guard<std::mutex> lock(zkb::g_knob_mutex);
+  zkb::Knob* k = zkb::find_knob(key);
+  if (!k || !value) return zkb::fail(ZKB_EINVAL, "unknown tuning knob '%s'", key ? key : "(null)");
+  *value = k->value;
+  return ZKB_OK;
+}
 
 int zkb_field_init(zkb_field* f, const uint64_t modulus[4]) {
   zkb::set_error("%s", "");

@@ -80,6 +80,8 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "zkb_msm_no_alloc": (ctypes.c_int, [_u64p, _u64p, _i64, ctypes.c_int, _u64p, _vp]),
     "zkb_msm_no_alloc_capacity": (ctypes.c_size_t, []),
     "zkb_launch_count": (ctypes.c_uint64, []),
+    "zkb_tune_set": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int]),
+    "zkb_tune_get": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)]),
     "zkb_profile_enable": (None, [ctypes.c_int]),
     "zkb_profile_report": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_size_t]),
 }
@@ -173,6 +175,17 @@ def make_field(modulus: int) -> ZkbField:
     f = ZkbField()
     check(lib().zkb_field_init(ctypes.byref(f), u64_array(limbs(modulus))), "zkb_field_init")
     return f
+
+
+def tune_set(key: str, value: int) -> None:
+    """Set a tuning knob of the library (see zkb_tune_set in include/zkb200.h)."""
+    check(lib().zkb_tune_set(key.encode(), int(value)), "zkb_tune_set")
+
+
+def tune_get(key: str) -> int:
+    v = ctypes.c_int(0)
+    check(lib().zkb_tune_get(key.encode(), ctypes.byref(v)), "zkb_tune_get")
+    return v.value
 
 
 def profile_enable(on: bool) -> None:
