@@ -306,19 +306,29 @@ __global__ void __launch_bounds__(kNttThreads, 1) k_ntt_pass(F f, NttPass a) {
     k1_0 = (bid >> a.lR2) << lc;
   }
 
-  // ---- load (bit-reversed into shared memory), with the coset pre-scale ----
+  // The stage table w_R^j (j < R/2) sits in shared memory after the columns.
+  uint64_t* tw = sm + (size_t)C * ((4 << lr) + 2);
+  for (int j = threadIdx.x; j < (R >> 1); j += blockDim.x) {
+    uint32_t w[8];
+    fe_load_nc(w, a.w + 4 * ((int64_t)j << (a.log_rmax - lr)));
+    fe_store(tw + 4 * j, w);
+  }
+
+  // ---- load, with the coset pre-scale: shared position jr holds input row
+  // brev(jr), so the bit reversal happens in the global gather and the
+  // shared-memory stores stay consecutive (no bank conflicts) ----
   for (int t = threadIdx.x; t < total; t += blockDim.x) {
-    int c, j;
-    int64_t pos;
+    int c, jr;
     if (!a.last) {
       c = t & (C - 1);
-      j = t >> lc;
-      pos = o * B + (int64_t)j * S + j0 + c;
+      jr = t >> lc;
     } else {
       c = t >> lr;
-      j = t & (R - 1);
-      pos = (((k1_0 + c) << a.lR2) + k2) * R + j;
+      jr = t & (R - 1);
     }
+    const int j = lr ? (int)(__brev((unsigned)jr) >> (32 - lr)) : 0;
+    const int64_t pos = !a.last ? o * B + (int64_t)j * S + j0 + c
+                                : (((k1_0 + c) << a.lR2) + k2) * R + j;
     uint32_t x[8];
     fe_load_nc(x, a.in + 4 * pos);
     if (a.first && a.g_lo && !a.inverse) {
@@ -329,31 +339,76 @@ __global__ void __launch_bounds__(kNttThreads, 1) k_ntt_pass(F f, NttPass a) {
       fe_mul(lo, lo, hi, f);
       fe_mul(x, x, lo, f);
     }
-    const int jr = lr ? (int)(__brev((unsigned)j) >> (32 - lr)) : 0;
     fe_store(sm + sm_index(c, jr, lr), x);
   }
   __syncthreads();
 
-  // ---- radix-2 DIT stages in shared memory ----
-  const int half_total = total >> 1;
-  for (int st = 0; st < lr; ++st) {
-    const int half = 1 << st;
+  // ---- DIT stages in shared memory, two per round trip (radix 4) ----
+  // A unit holds rows i0, i0 + h, i0 + 2h, i0 + 3h (h = 2^st, i0 = g 4h + jj):
+  // stage st pairs (i0, i0 + h) and (i0 + 2h, i0 + 3h) with w_2h^jj; stage
+  // st + 1 pairs (i0, i0 + 2h) with w_4h^jj and (i0 + h, i0 + 3h) with
+  // w_4h^(jj + h). In the first round jj = 0, so only w_4 multiplies.
+  int st = 0;
+  for (; st + 1 < lr; st += 2) {
+    const int h = 1 << st;
+    const int units = total >> 2;
+    for (int u = threadIdx.x; u < units; u += blockDim.x) {
+      const int c = u >> (lr - 2);
+      const int q = u & ((R >> 2) - 1);
+      const int jj = q & (h - 1);
+      const int i0 = ((q >> st) << (st + 2)) | jj;
+      uint32_t x0[8], x1[8], x2[8], x3[8], w[8], t[8];
+      fe_load(x0, sm + sm_index(c, i0, lr));
+      fe_load(x1, sm + sm_index(c, i0 + h, lr));
+      fe_load(x2, sm + sm_index(c, i0 + 2 * h, lr));
+      fe_load(x3, sm + sm_index(c, i0 + 3 * h, lr));
+      if (st > 0) {
+        fe_load(w, tw + 4 * (jj << (lr - 1 - st)));  // w_2h^jj
+        fe_mul(x1, x1, w, f);
+        fe_mul(x3, x3, w, f);
+      }
+      fe_add(t, x0, x1, f);
+      fe_sub(x1, x0, x1, f);
+      fe_copy(x0, t);
+      fe_add(t, x2, x3, f);
+      fe_sub(x3, x2, x3, f);
+      fe_copy(x2, t);
+      if (st > 0) {
+        fe_load(w, tw + 4 * (jj << (lr - 2 - st)));  // w_4h^jj
+        fe_mul(x2, x2, w, f);
+      }
+      fe_load(w, tw + 4 * ((jj + h) << (lr - 2 - st)));  // w_4h^(jj + h)
+      fe_mul(x3, x3, w, f);
+      fe_add(t, x0, x2, f);
+      fe_sub(x2, x0, x2, f);
+      fe_store(sm + sm_index(c, i0, lr), t);
+      fe_store(sm + sm_index(c, i0 + 2 * h, lr), x2);
+      fe_add(t, x1, x3, f);
+      fe_sub(x3, x1, x3, f);
+      fe_store(sm + sm_index(c, i0 + h, lr), t);
+      fe_store(sm + sm_index(c, i0 + 3 * h, lr), x3);
+    }
+    __syncthreads();
+  }
+  if (st < lr) {  // an odd number of stages: one radix-2 stage left
+    const int h = 1 << st;
+    const int half_total = total >> 1;
     for (int b = threadIdx.x; b < half_total; b += blockDim.x) {
       const int c = b >> (lr - 1);
       const int k = b & ((R >> 1) - 1);
-      const int jj = k & (half - 1);
+      const int jj = k & (h - 1);
       const int i0 = ((k >> st) << (st + 1)) | jj;
-      const int i1 = i0 + half;
-      uint32_t u[8], v[8], w[8];
+      uint32_t u[8], v[8], w[8], x[8];
       fe_load(u, sm + sm_index(c, i0, lr));
-      fe_load(v, sm + sm_index(c, i1, lr));
-      fe_load_nc(w, a.w + 4 * ((int64_t)jj << (a.log_rmax - 1 - st)));
-      fe_mul(v, v, w, f);
-      uint32_t x[8];
+      fe_load(v, sm + sm_index(c, i0 + h, lr));
+      if (st > 0) {
+        fe_load(w, tw + 4 * (jj << (lr - 1 - st)));
+        fe_mul(v, v, w, f);
+      }
       fe_add(x, u, v, f);
       fe_sub(v, u, v, f);
       fe_store(sm + sm_index(c, i0, lr), x);
-      fe_store(sm + sm_index(c, i1, lr), v);
+      fe_store(sm + sm_index(c, i0 + h, lr), v);
     }
     __syncthreads();
   }
@@ -548,7 +603,8 @@ static int run_ntt(const F& f, const zkb_field* field, const uint64_t* in, uint6
       ctas = n >> (a.lr + lc);
     }
     a.lc = lc;
-    const size_t smem = (size_t)(1 << lc) * ((32u << a.lr) + 16);
+    // padded columns, then the stage table (R / 2 rows)
+    const size_t smem = (size_t)(1 << lc) * ((32u << a.lr) + 16) + ((size_t)16 << a.lr);
     auto kern = k_ntt_pass<F>;
     ZKB_TRY(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)smem),
