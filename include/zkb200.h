@@ -185,8 +185,13 @@ size_t zkb_msm_no_alloc_capacity(void);
 
 /* Tuning knobs, read by each call when it plans its work (so they also change
  * the workspace size queries): "msm.pairs_per_thread" (default 64),
- * "msm.slots_per_thread" (8), "msm.reduce_log_segment" (2). ZKB_EINVAL for
- * an unknown name or a value out of range. Process-wide, not per stream. */
+ * "msm.slots_per_thread" (8), "msm.reduce_log_segment" (2),
+ * "ntt.max_log_radix" (12, range 8..12: the largest sub-transform one NTT pass
+ * does), "ntt.cta_log_elems" (log2 of the rows staged per NTT block, 9..12;
+ * default 0 = 12 for large transforms, 10 when fewer than four 4096-row
+ * blocks per SM), "ntt.threads" (threads per NTT block, 64..512; default 0 =
+ * 512 for 4096-row blocks, else 256). ZKB_EINVAL for an unknown name or a
+ * value out of range. Process-wide, not per stream. */
 int zkb_tune_set(const char* key, int value);
 int zkb_tune_get(const char* key, int* value);
 

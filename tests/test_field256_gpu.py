@@ -199,6 +199,47 @@ def test_ntt_matches_c_oracle_between_fixture_sizes(log_n):
             assert np.array_equal(got, want), (invert, coset)
 
 
+@pytest.mark.parametrize(
+    "knobs",
+    [
+        {"ntt.max_log_radix": 8},  # three passes at 2^20 and above
+        {"ntt.max_log_radix": 9, "ntt.cta_log_elems": 9, "ntt.threads": 64},
+        {"ntt.cta_log_elems": 12, "ntt.threads": 128},
+        {"ntt.cta_log_elems": 10, "ntt.threads": 512},
+    ],
+)
+def test_ntt_pass_plans_give_the_same_rows(knobs):
+    """Every pass split, tile size and block size the tuning knobs allow computes the same rows
+    (against the reference's digests at 2^16 and 2^20, and the C oracle at 2^13 and 2^21)."""
+    from zkgpu import _native
+
+    try:
+        for k, v in knobs.items():
+            _native.tune_set(k, v)
+        for n in ("65536", "1048576"):
+            entry = golden("ntt.json")["large"].get(n)
+            if entry is None:
+                continue
+            rows = BN254_FR.to_montgomery(wl.uniform_fr(entry["seed"], int(n)))
+            assert digest(BN254_FR.ntt(rows)) == entry["fwd_sha256"], n
+            assert digest(BN254_FR.ntt(rows, invert=True)) == entry["inv_sha256"], n
+            if "coset_fwd_sha256" in entry:
+                assert digest(BN254_FR.ntt(rows, coset=5)) == entry["coset_fwd_sha256"], n
+                assert digest(BN254_FR.ntt(rows, coset=5, invert=True)) == entry["coset_inv_sha256"], n
+        for log_n in (13, 21):
+            n = 1 << log_n
+            rows = BN254_FR.to_montgomery(wl.uniform_fr(60 + log_n, n))
+            host = co.to_mont(co.FR, wl.uniform_fr(60 + log_n, n))
+            for invert, coset in ((False, None), (True, 5)):
+                want = co.ntt(host, invert=invert, coset=coset, threads=os.cpu_count() or 1)
+                got = BN254_FR.ntt(rows, invert=invert, coset=coset).cpu().numpy()
+                assert np.array_equal(got, want), (log_n, invert, coset)
+    finally:
+        _native.tune_set("ntt.max_log_radix", 12)
+        _native.tune_set("ntt.cta_log_elems", 0)
+        _native.tune_set("ntt.threads", 0)
+
+
 def test_ntt_2_24_config_size():
     """Config 3's NTT: 2^24 elements (512 MiB), plain and coset g = 5, against the C oracle,
     plus the size-independent round trips."""

@@ -80,7 +80,8 @@ def test_status_codes_map_to_reference_exceptions():
 
 def test_host_only_queries():
     lib = _native.lib()
-    assert lib.zkb_ntt_workspace_bytes(4096) == 0
+    assert lib.zkb_ntt_workspace_bytes(512) == 0  # one pass, no intermediate rows
+    assert lib.zkb_ntt_workspace_bytes(4096) == 4096 * 32  # split in two passes from 2^10 on
     assert lib.zkb_ntt_workspace_bytes(1 << 20) == 32 << 20
     # default window: argmin of windows * (20 n + 42 * 2^(w-1)): signed digits over
     # the two 127-bit GLV halves, ceil(128 / w) windows
@@ -89,6 +90,26 @@ def test_host_only_queries():
         return best if n > 1 else 1
     for n in (1, 100, 2**12, 2**16, 2**20, 2**22):
         assert lib.zkb_msm_default_window(n) == model(n), n
+
+
+def test_tuning_knobs_validate_and_plan_the_workspace():
+    defaults = {"msm.pairs_per_thread": 64, "msm.slots_per_thread": 8, "msm.reduce_log_segment": 2,
+                "ntt.max_log_radix": 12, "ntt.cta_log_elems": 0, "ntt.threads": 0}
+    assert {k: _native.tune_get(k) for k in defaults} == defaults
+    with pytest.raises(ValueError, match="unknown tuning knob"):
+        _native.tune_set("ntt.bogus", 1)
+    with pytest.raises(ValueError, match="8..12"):
+        _native.tune_set("ntt.max_log_radix", 13)
+    lib = _native.lib()
+    try:
+        # at most 8 bits per pass: 2^9 rows no longer fit one pass
+        _native.tune_set("ntt.max_log_radix", 8)
+        assert lib.zkb_ntt_workspace_bytes(1 << 20) == 32 << 20
+        assert lib.zkb_ntt_workspace_bytes(512) == 512 * 32
+        assert lib.zkb_ntt_workspace_bytes(256) == 0
+    finally:
+        _native.tune_set("ntt.max_log_radix", 12)
+    assert lib.zkb_ntt_workspace_bytes(512) == 0
 
 
 def test_gpu_entry_points_reject_bad_arguments_before_touching_the_device():

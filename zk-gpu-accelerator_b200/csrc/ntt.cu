@@ -29,7 +29,6 @@
 namespace zkb {
 
 static constexpr int kMaxLogR = 12;                 // largest sub-transform: 4096 points
-static constexpr int kMaxCtaElems = 1 << kMaxLogR;  // elements staged per CTA
 static constexpr int kNttThreads = 512;
 static constexpr int kMaxLogN = 28;
 
@@ -266,7 +265,10 @@ struct NttPass {
 // Shared-memory address (in uint64 units) of element j of column c: columns
 // are padded by 16 bytes so that consecutive columns start in different banks.
 __device__ __forceinline__ int sm_index(int c, int j, int lr) {
-  return c * ((4 << lr) + 2) + 4 * j;
+  // XOR swizzle within each 128-byte row of four elements: the radix-4 rounds
+  // with a small span (h = 1, 4, 16) touch rows 4h apart, which without it
+  // would all fall into the same banks.
+  return c * ((4 << lr) + 2) + 4 * (j ^ ((j >> 2) & 3));
 }
 
 template <class F>
@@ -463,17 +465,30 @@ static int ilog2(int64_t n) {
   return l;
 }
 
-size_t workspace_bytes(int64_t n) {
-  if (n <= (1ll << kMaxLogR)) return 0;
-  return (size_t)n * 32;
-}
-
-// Splits log_n into P parts of at most kMaxLogR bits, the larger parts first.
+// Splits log_n into P parts of at most "ntt.max_log_radix" bits (at most 12,
+// the shared-memory limit), the larger parts first. At most three passes:
+// the last pass's output mapping covers P <= 3, which 12-bit passes reach up
+// to 2^36. From 2^10 rows on, a transform that fits one pass is still split
+// in two: one pass would be a single CTA on one SM, while two passes of
+// 2^5..2^6-point sub-transforms spread it over 32-64 CTAs (2^12 rows: 0.048
+// ms instead of 0.11 ms on a B200).
 static std::vector<int> plan_radices(int log_n) {
-  const int P = (log_n + kMaxLogR - 1) / kMaxLogR;
+  const int max_r = tune_get("ntt.max_log_radix");
+  int P = (log_n + max_r - 1) / max_r;
+  if (P > 3) P = 3;
+  if (P < (log_n + kMaxLogR - 1) / kMaxLogR) P = (log_n + kMaxLogR - 1) / kMaxLogR;
+  if (P < 2 && log_n >= 10) P = 2;
+  if (P < 1) P = 1;
   std::vector<int> r(P, log_n / P);
   for (int q = 0; q < log_n % P; ++q) r[q] += 1;
   return r;
+}
+
+size_t workspace_bytes(int64_t n) {
+  int log_n = 0;
+  while ((1ll << log_n) < n) ++log_n;
+  if (n <= 1 || plan_radices(log_n).size() == 1) return 0;
+  return (size_t)n * 32;
 }
 
 template <class F>
@@ -561,6 +576,9 @@ static int run_ntt(const F& f, const zkb_field* field, const uint64_t* in, uint6
                 (long long)n, workspace_bytes(n), ws_bytes);
   }
 
+  int sms = 0;
+  ZKB_TRY(check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, key.device),
+                     "SM count"));
   int ls = log_n;  // stride exponent of the current pass: S_q = 2^(log_n - sum of radices so far)
   for (int q = 0; q < P; ++q) {
     NttPass a;
@@ -584,20 +602,26 @@ static int run_ntt(const F& f, const zkb_field* field, const uint64_t* in, uint6
     a.g_hi = st.g_hi;
     a.gs = st.gs;
     a.scale = st.scale;
-    int lc;
+    // columns per CTA: the tile C R is at most 2^"ntt.cta_log_elems" elements.
+    // Auto (0): 4096-row tiles of 512 threads (one CTA per SM, 128 KiB of
+    // shared memory) when that gives at least 16 CTAs per SM (2^24 rows and
+    // up on a B200), else 1024-row tiles of 256 threads, several per SM,
+    // which measured faster from 2^12 to 2^22 rows.
+    int cta_log = tune_get("ntt.cta_log_elems");
+    int threads = tune_get("ntt.threads");
+    if (cta_log < 9) cta_log = (n >> kMaxLogR) >= 16 * sms ? kMaxLogR : 10;
+    if (threads < 64) threads = cta_log >= kMaxLogR ? 512 : 256;
+    int lc = cta_log > a.lr ? cta_log - a.lr : 0;
     int64_t ctas;
     if (!a.last) {
-      lc = kMaxLogR - a.lr;
       if (lc > a.ls) lc = a.ls;
       ctas = n >> (a.lr + lc);
     } else {
-      // R1 = first radix, R2 = product of the middle radices (P = 3 at most
-      // for n <= 2^28 with 4096-point passes, so R2 is radices[1] then).
+      // R1 = first radix, R2 = the middle radix (P <= 3)
       const int lR1 = radices[0];
       const int lR2 = P >= 3 ? radices[1] : 0;
       a.lR1 = P >= 2 ? lR1 : 0;
       a.lR2 = lR2;
-      lc = kMaxLogR - a.lr;
       const int k1_bits = P >= 2 ? lR1 : 0;
       if (lc > k1_bits) lc = k1_bits;
       ctas = n >> (a.lr + lc);
@@ -609,7 +633,6 @@ static int run_ntt(const F& f, const zkb_field* field, const uint64_t* in, uint6
     ZKB_TRY(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)smem),
                        "NTT shared memory attribute"));
-    int threads = kNttThreads;
     const int half_total = (1 << (a.lr + lc)) >> 1;
     if (half_total < threads) threads = half_total < 32 ? 32 : half_total;
     {
