@@ -108,6 +108,30 @@ int zkb_ntt(const zkb_field* f, const uint64_t* in, uint64_t* out, int64_t n, in
             const uint64_t* omega, const uint64_t* coset, void* workspace,
             size_t workspace_bytes, void* stream);
 
+/* One transform of a batch (device pointers). */
+typedef struct zkb_ntt_job {
+  const uint64_t* in; /* (n, 4) Montgomery rows; not modified */
+  uint64_t* out;      /* (n, 4); must not alias any input of the batch */
+  int64_t n;          /* a power of two, 0 <= n <= 2^28 */
+  int32_t invert;     /* nonzero: inverse transform */
+  int32_t has_coset;  /* nonzero: coset transform with offset `coset` */
+  uint64_t coset[4];  /* plain value of the coset offset g */
+} zkb_ntt_job;
+
+/* Device workspace (bytes) zkb_ntt_batch needs for these jobs (host array). */
+size_t zkb_ntt_batch_workspace_bytes(const zkb_ntt_job* jobs, int count);
+
+/* Batched form of zkb_ntt over BN254 Fr (built-in roots 5^((r-1)/n)): up to 64
+ * independent transforms of any sizes in ONE persistent kernel launch. The
+ * launch's CTAs take CTA-sized tiles from a device counter, first passes of
+ * all transforms before second passes; a tile of a later pass waits for the
+ * previous pass of its own transform (a bounded wait). Each job's output is
+ * bit-identical to zkb_ntt's for the same arguments. `status` (device int32,
+ * may be NULL) receives ZKB_OK, or ZKB_ETIMEOUT if a wait gave up (outputs
+ * are then incomplete). `jobs` is a host array, read during the call. */
+int zkb_ntt_batch(const zkb_field* f, const zkb_ntt_job* jobs, int count, void* workspace,
+                  size_t workspace_bytes, int32_t* status, void* stream);
+
 /* ---- BN254 G1 ------------------------------------------------------------- */
 
 /* Replace the zk_g1_add / zk_g1_add_affine / zk_g1_double launches
@@ -180,6 +204,32 @@ int zkb_msm_no_alloc(const uint64_t* points, const uint64_t* scalars, int64_t n,
 
 /* Size in bytes of the fixed scratch array zkb_msm_no_alloc works in. */
 size_t zkb_msm_no_alloc_capacity(void);
+
+/* One MSM of a batch: the arguments of zkb_msm (device pointers). */
+typedef struct zkb_msm_job {
+  const uint64_t* points;  /* (n, 2, 4) affine, Montgomery form */
+  const uint64_t* scalars; /* (n, 4) plain 256-bit integers */
+  int64_t n;               /* 0 <= n < 2^30; n = 0 gives infinity */
+  uint64_t* result;        /* 9 uint64, laid out as zkb_msm's */
+  int32_t window_size;     /* 1..20, or 0 for zkb_msm_default_window(n) */
+  int32_t reserved;
+} zkb_msm_job;
+
+/* Device workspace (bytes) zkb_msm_batch needs for these jobs (host array). */
+size_t zkb_msm_batch_workspace_bytes(const zkb_msm_job* jobs, int count);
+
+/* Batched form of msm_pippenger_gpu (zkgpu/msm_gpu.py:398-449) for many
+ * independent MSMs of uneven sizes, e.g. the four G1 MSMs of a Groth16 proof
+ * (demo/prover_simulation.py:94-98) or MSMs over prefixes of one resident
+ * base set. Each job's result is exactly zkb_msm's for the same arguments.
+ * Jobs with the same window size run through one pipeline (one sort, one
+ * bucket pass, one reduction and one finalize for all of them, up to 64 jobs
+ * and 2^31 digit pairs per group); groups of different window sizes run
+ * concurrently on library-owned side streams that fork from and join back to
+ * `stream`. `jobs` is a host array; nothing is copied from it after the call
+ * returns. */
+int zkb_msm_batch(const zkb_msm_job* jobs, int count, void* workspace, size_t workspace_bytes,
+                  void* stream);
 
 /* ---- measurement -------------------------------------------------------- */
 

@@ -112,6 +112,33 @@ def test_tuning_knobs_validate_and_plan_the_workspace():
     assert lib.zkb_ntt_workspace_bytes(512) == 0
 
 
+def test_batch_entry_points_validate_on_the_host():
+    lib = _native.lib()
+    jobs = (_native.ZkbNttJob * 65)()
+    for j in range(65):
+        jobs[j].n = 8
+    # counters (256 B) + 192 pass counters, then 2^12 rows of intermediate storage
+    jobs[0].n, jobs[1].n = 4096, 8
+    assert lib.zkb_ntt_batch_workspace_bytes(jobs, 2) == 1024 + 4096 * 32
+    assert lib.zkb_ntt_batch_workspace_bytes(jobs, 65) == 0
+    assert "0..64" in _native.last_error()
+    fr, fq = _native.make_field(R), _native.make_field(P)
+    assert lib.zkb_ntt_batch(ctypes.byref(fq), jobs, 2, None, 0, None, None) == _native.ZKB_EINVAL
+    assert "BN254 Fr" in _native.last_error()
+    jobs[1].n = 6
+    assert lib.zkb_ntt_batch(ctypes.byref(fr), jobs, 2, None, 0, None, None) == _native.ZKB_EINVAL
+    assert "power of 2" in _native.last_error()
+    jobs[1].n = 8
+    assert lib.zkb_ntt_batch(ctypes.byref(fr), jobs, 2, None, 0, None, None) == _native.ZKB_EWORKSPACE
+    msm = (_native.ZkbMsmJob * 2)()
+    msm[0].n, msm[0].result = -1, 64
+    assert lib.zkb_msm_batch(msm, 2, None, 0, None) == _native.ZKB_EINVAL
+    assert "negative point count" in _native.last_error()
+    msm[0].n, msm[0].window_size = 4, 21
+    assert lib.zkb_msm_batch_workspace_bytes(msm, 1) == 0
+    assert "window_size" in _native.last_error()
+
+
 def test_gpu_entry_points_reject_bad_arguments_before_touching_the_device():
     lib = _native.lib()
     f = _native.make_field(R)

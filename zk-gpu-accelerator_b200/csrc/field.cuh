@@ -100,6 +100,15 @@ __device__ __forceinline__ void fe_load_nc(uint32_t r[8], const void* src) {
   r[4] = hi.x; r[5] = hi.y; r[6] = hi.z; r[7] = hi.w;
 }
 
+// Data written earlier in the same kernel by other CTAs: cached in L2 only,
+// so that no stale L1 line of this SM is read.
+__device__ __forceinline__ void fe_load_cg(uint32_t r[8], const void* src) {
+  const uint4* s = reinterpret_cast<const uint4*>(src);
+  uint4 lo = __ldcg(s), hi = __ldcg(s + 1);
+  r[0] = lo.x; r[1] = lo.y; r[2] = lo.z; r[3] = lo.w;
+  r[4] = hi.x; r[5] = hi.y; r[6] = hi.z; r[7] = hi.w;
+}
+
 __device__ __forceinline__ void fe_store(void* dst, const uint32_t a[8]) {
   uint4* d = reinterpret_cast<uint4*>(dst);
   d[0] = make_uint4(a[0], a[1], a[2], a[3]);

@@ -29,10 +29,13 @@
 // and the last term is the same problem on the L S_t with delta = 0.
 #include <cub/device/device_radix_sort.cuh>
 
+#include <algorithm>
+#include <cstring>
 #include <mutex>
 #include <vector>
 
 #include "curve.cuh"
+#include "fanout.h"
 #include "field_host.h"
 #include "profile.h"
 
@@ -198,11 +201,41 @@ __device__ __forceinline__ void glv_split(const uint32_t k[8], uint32_t k1[4], u
 }
 
 // ---------------------------------------------------------------------------
+// Batches: several independent MSMs with one window size run through one
+// pipeline. Job j's buckets take keys [j K, (j + 1) K) with K = W 2^(w-1), so
+// "window" j W + win of the batch is window win of job j: the sort, the
+// bucket levels and the reduction see one MSM with count * W windows, and
+// only the digits, the point lookups and the finalize know about jobs. The
+// table travels as a kernel parameter (2.6 KB), so a batch needs no host to
+// device copy and can be captured in a CUDA graph.
+// ---------------------------------------------------------------------------
+
+static constexpr int kMsmMaxBatch = 64;
+
+struct MsmJobs {
+  int count;
+  uint32_t keys_per_job;              // W 2^(w-1)
+  int64_t first[kMsmMaxBatch + 1];    // prefix sums of the jobs' point counts
+  const uint64_t* points[kMsmMaxBatch];
+  const uint64_t* scalars[kMsmMaxBatch];
+  uint64_t* phi[kMsmMaxBatch];        // phi images, in the workspace
+  uint64_t* result[kMsmMaxBatch];
+};
+
+// The job holding batch-wide point index i (first[j] <= i < first[j + 1]).
+__device__ __forceinline__ int job_of_point(const MsmJobs& J, int64_t i) {
+  int lo = 0, hi = J.count - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (J.first[mid] <= i) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// ---------------------------------------------------------------------------
 // 1. digits
 // ---------------------------------------------------------------------------
 
-// Bits [lo, lo + w) of a 256-bit little-endian value (w <= 20 spans two limbs
-// at most).
 // Bits [lo, lo + w) of a 128-bit little-endian magnitude (w <= 20, so at most
 // two limbs; bits at and above 128 are zero).
 __device__ __forceinline__ uint32_t half_bits(const uint32_t s[4], int lo, int w) {
@@ -214,10 +247,12 @@ __device__ __forceinline__ uint32_t half_bits(const uint32_t s[4], int lo, int w
 }
 
 // Signed w-bit digits of one GLV half |k| (sign neg) of point `point`: the pair
-// (key, value) for window win goes to entry (half * W + win) * n + i.
+// (key, value) for window win goes to entry first_entry + win * n, its key is
+// key_base + win 2^(w-1) + |d| - 1.
 __device__ __forceinline__ void emit_digits(const uint32_t k[4], uint32_t neg, uint32_t point,
                                             int64_t first_entry, int64_t n, int w, int W,
-                                            uint32_t none, uint32_t* keys, uint32_t* vals) {
+                                            uint32_t key_base, uint32_t none, uint32_t* keys,
+                                            uint32_t* vals) {
   const uint32_t half = 1u << (w - 1);
   uint32_t carry = 0;
   for (int win = 0; win < W; ++win) {
@@ -237,43 +272,52 @@ __device__ __forceinline__ void emit_digits(const uint32_t k[4], uint32_t neg, u
       keys[e] = none;
       vals[e] = 0;
     } else {
-      keys[e] = ((uint32_t)win << (w - 1)) | (mag - 1);
+      keys[e] = key_base + (((uint32_t)win << (w - 1)) | (mag - 1));
       vals[e] = point | ((neg ^ dneg) << 31);
     }
   }
 }
 
-// One thread per scalar: reduce mod r, split k = k1 + k2 lambda, and emit the
-// digits of k1 (points 0..n-1) and of k2 (points n..2n-1, the phi images).
-__global__ void __launch_bounds__(256) k_msm_digits(const uint64_t* scalars, int64_t n, int w,
-                                                    int W, uint32_t none, uint32_t* keys,
-                                                    uint32_t* vals) {
+// One thread per scalar of the batch: reduce mod r, split k = k1 + k2 lambda,
+// and emit the digits of k1 (the job's points 0..n-1) and of k2 (its points
+// n..2n-1, the phi images). Job j's 2 W n_j entries start at 2 W first[j].
+__global__ void __launch_bounds__(256) k_msm_digits(const MsmJobs J, int w, int W, uint32_t none,
+                                                    uint32_t* keys, uint32_t* vals) {
   FrP fr;
+  const int64_t N = J.first[J.count];
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < N; g += stride) {
+    const int j = job_of_point(J, g);
+    const int64_t n = J.first[j + 1] - J.first[j], i = g - J.first[j];
+    const int64_t base = 2 * (int64_t)W * J.first[j];
+    const uint32_t key_base = (uint32_t)j * J.keys_per_job;
     uint32_t s[8];
-    fe_load_nc(s, scalars + 4 * i);
+    fe_load_nc(s, J.scalars[j] + 4 * i);
     fe_reduce_full(s, fr, 5);  // any 256-bit value -> [0, r)
     uint32_t k1[4], k2[4], neg1, neg2;
     glv_split(s, k1, neg1, k2, neg2);
-    emit_digits(k1, neg1, (uint32_t)i, i, n, w, W, none, keys, vals);
-    emit_digits(k2, neg2, (uint32_t)(n + i), (int64_t)W * n + i, n, w, W, none, keys, vals);
+    emit_digits(k1, neg1, (uint32_t)i, base + i, n, w, W, key_base, none, keys, vals);
+    emit_digits(k2, neg2, (uint32_t)(n + i), base + (int64_t)W * n + i, n, w, W, key_base, none,
+                keys, vals);
   }
 }
 
 // phi(P_i) = (beta x_i, y_i), the points that the k2 halves multiply.
-__global__ void __launch_bounds__(256) k_msm_phi(const uint64_t* points, int64_t n, uint64_t* phi) {
+__global__ void __launch_bounds__(256) k_msm_phi(const MsmJobs J) {
   FqP f;
   uint32_t beta[8];
   glv_beta_mont(beta);
+  const int64_t N = J.first[J.count];
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < N; g += stride) {
+    const int j = job_of_point(J, g);
+    const int64_t i = g - J.first[j];
     uint32_t x[8], y[8];
-    fe_load_nc(x, points + 8 * i);
-    fe_load_nc(y, points + 8 * i + 4);
+    fe_load_nc(x, J.points[j] + 8 * i);
+    fe_load_nc(y, J.points[j] + 8 * i + 4);
     fe_mul(x, x, beta, f);
-    fe_store(phi + 8 * i, x);
-    fe_store(phi + 8 * i + 4, y);
+    fe_store(J.phi[j] + 8 * i, x);
+    fe_store(J.phi[j] + 8 * i + 4, y);
   }
 }
 
@@ -328,14 +372,26 @@ struct RunSink {
   }
 };
 
+// The points of the job that owns bucket key `key`.
+struct JobPoints {
+  const uint64_t* points;
+  const uint64_t* phi;
+  int64_t n;
+};
+
+__device__ __forceinline__ JobPoints job_points(const MsmJobs& J, uint32_t key) {
+  const int j = (int)(key / J.keys_per_job);
+  return JobPoints{J.points[j], J.phi[j], J.first[j + 1] - J.first[j]};
+}
+
 // Level 1: K1 sorted (key, value) pairs per thread, mixed additions of affine
-// input points.
-__global__ void __launch_bounds__(128) k_msm_acc_points(const uint64_t* points,
-                                                        const uint64_t* phi, int64_t n,
-                                                        const uint32_t* keys,
-                                                        const uint32_t* vals, int64_t E, int K,
-                                                        uint32_t none, uint64_t* buckets,
-                                                        uint32_t* slot_keys, uint64_t* slot_pts) {
+// input points. kBatch = false is the one-job form: the job lookup at each
+// new run costs 40+ registers, so a single MSM keeps its point arrays fixed.
+template <bool kBatch>
+__device__ __forceinline__ void acc_points(const MsmJobs& J, const uint32_t* keys,
+                                           const uint32_t* vals, int64_t E, int K, uint32_t none,
+                                           uint64_t* buckets, uint32_t* slot_keys,
+                                           uint64_t* slot_pts) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t T = (E + K - 1) / K;
   if (t >= T) return;
@@ -349,6 +405,7 @@ __global__ void __launch_bounds__(128) k_msm_acc_points(const uint64_t* points,
   bool first = true;
   Xyzz acc;
   xyzz_set_identity(acc);
+  JobPoints jp = job_points(J, (!kBatch || cur == none) ? 0 : cur);
   for (int64_t e = start; e < end; ++e) {
     const uint32_t k = keys[e];
     if (k != cur) {
@@ -356,16 +413,37 @@ __global__ void __launch_bounds__(128) k_msm_acc_points(const uint64_t* points,
       first = false;
       xyzz_set_identity(acc);
       cur = k;
+      if (kBatch && k != none) jp = job_points(J, k);
     }
     if (k == none) break;  // zero digits sort last: nothing after them
     const uint32_t v = vals[e];
     const int64_t idx = (int64_t)(v & 0x7fffffffu);
     Aff q;
-    aff_load_nc(q, idx < n ? points + 8 * idx : phi + 8 * (idx - n));
+    aff_load_nc(q, idx < jp.n ? jp.points + 8 * idx : jp.phi + 8 * (idx - jp.n));
     if (v >> 31) aff_neg(q);
     xyzz_add_affine(acc, q);
   }
   if (cur != none) sink.flush(cur, acc, first, true);
+}
+
+// One MSM (108 registers, four CTAs per SM).
+__global__ void __launch_bounds__(128) k_msm_acc_points(const MsmJobs J, const uint32_t* keys,
+                                                        const uint32_t* vals, int64_t E, int K,
+                                                        uint32_t none, uint64_t* buckets,
+                                                        uint32_t* slot_keys, uint64_t* slot_pts) {
+  acc_points<false>(J, keys, vals, E, K, none, buckets, slot_keys, slot_pts);
+}
+
+// A batch: capped at 128 registers (a few bytes of spill on the job-change
+// path) to keep four CTAs per SM.
+__global__ void __launch_bounds__(128, 4) k_msm_acc_points_batch(const MsmJobs J,
+                                                                 const uint32_t* keys,
+                                                                 const uint32_t* vals, int64_t E,
+                                                                 int K, uint32_t none,
+                                                                 uint64_t* buckets,
+                                                                 uint32_t* slot_keys,
+                                                                 uint64_t* slot_pts) {
+  acc_points<true>(J, keys, vals, E, K, none, buckets, slot_keys, slot_pts);
 }
 
 // Levels 2+: K2 slots per thread, full XYZZ additions; slots without a key
@@ -445,9 +523,14 @@ __global__ void __launch_bounds__(128) k_msm_reduce(const uint64_t* X, const uin
 // 5. finalize
 // ---------------------------------------------------------------------------
 
-// Horner from the top window: acc = 2^w acc + S_win; then affine x = X / ZZ,
-// y = Y / ZZZ with one inversion of ZZ ZZZ, as plain canonical values.
-__global__ void k_msm_finalize(const uint64_t* window_sums, int W, int w, uint64_t* result) {
+// One thread per job. Horner from the top window: acc = 2^w acc + S_win; then
+// affine x = X / ZZ, y = Y / ZZZ with one inversion of ZZ ZZZ, as plain
+// canonical values.
+__global__ void k_msm_finalize(const MsmJobs J, const uint64_t* all_window_sums, int W, int w) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= J.count) return;
+  const uint64_t* window_sums = all_window_sums + 16 * (int64_t)j * W;
+  uint64_t* result = J.result[j];
   G1F f;
   Xyzz acc, s;
   xyzz_load(acc, window_sums + 16 * (W - 1));
@@ -513,7 +596,9 @@ int default_window(int64_t n) {
 static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 struct MsmPlan {
-  int64_t n = 0;
+  int count = 1;                // jobs in the batch (all at window w)
+  std::vector<int64_t> first;   // prefix sums of the jobs' point counts
+  int64_t n = 0;                // points of all jobs
   int w = 0, W = 0, key_bits = 0;
   uint32_t none = 0;
   int64_t nb = 0;  // buckets per window
@@ -530,12 +615,17 @@ struct MsmPlan {
       off_red_s1, off_red_u1, off_wsum, total;
 };
 
-static int make_plan(int64_t n, int w, MsmPlan& p) {
+// Plan for a batch of jobs with point counts sizes[0..count) at window w.
+static int make_plan(const int64_t* sizes, int count, int w, MsmPlan& p) {
+  p.count = count;
+  p.first.assign(count + 1, 0);
+  for (int j = 0; j < count; ++j) p.first[j + 1] = p.first[j] + sizes[j];
+  const int64_t n = p.first[count];
   p.n = n;
   p.w = w;
   p.W = num_windows(w);
   p.nb = 1ll << (w - 1);
-  const int64_t keys_used = (int64_t)p.W * p.nb;
+  const int64_t keys_used = (int64_t)count * p.W * p.nb;
   int bits = 1;
   while ((1ll << bits) <= keys_used) ++bits;  // keys_used itself must fit below none
   p.key_bits = bits;
@@ -573,38 +663,55 @@ static int make_plan(int64_t n, int w, MsmPlan& p) {
   p.off_vals1 = take((size_t)p.E * 4);
   p.off_cub = take(p.cub_bytes);
   p.off_phi = take((size_t)n * 64);
-  p.off_buckets = take((size_t)p.W * p.nb * 128);
+  const int64_t windows = (int64_t)count * p.W;  // the batch's windows
+  p.off_buckets = take((size_t)windows * p.nb * 128);
   p.off_slot_keys_a = take((size_t)2 * p.T1 * 4);
   p.off_slot_pts_a = take((size_t)2 * p.T1 * 128);
   const int64_t second = p.slot_levels.empty() ? 1 : p.slot_levels[0];
   p.off_slot_keys_b = take((size_t)2 * second * 4);
   p.off_slot_pts_b = take((size_t)2 * second * 128);
-  const int64_t red = (int64_t)p.W * (p.nb >> p.log_l > 0 ? p.nb >> p.log_l : 1);
+  const int64_t red = windows * (p.nb >> p.log_l > 0 ? p.nb >> p.log_l : 1);
   p.off_red_s0 = take((size_t)red * 128);
   p.off_red_u0 = take((size_t)red * 128);
   p.off_red_s1 = take((size_t)red * 128);
   p.off_red_u1 = take((size_t)red * 128);
-  p.off_wsum = take((size_t)p.W * 128);
+  p.off_wsum = take((size_t)windows * 128);
   p.total = off;
   return ZKB_OK;
 }
 
-static int run_msm(const uint64_t* points, const uint64_t* scalars, const MsmPlan& p,
-                   uint64_t* result, char* ws, cudaStream_t s) {
+// The kernel-parameter job table of a planned batch.
+static MsmJobs job_table(const MsmPlan& p, const uint64_t* const* points,
+                         const uint64_t* const* scalars, uint64_t* const* results, char* ws) {
+  MsmJobs J;
+  std::memset(&J, 0, sizeof J);
+  J.count = p.count;
+  J.keys_per_job = (uint32_t)(p.W * p.nb);
+  uint64_t* phi = reinterpret_cast<uint64_t*>(ws + p.off_phi);
+  for (int j = 0; j <= p.count; ++j) J.first[j] = p.first[j];
+  for (int j = 0; j < p.count; ++j) {
+    J.points[j] = points[j];
+    J.scalars[j] = scalars[j];
+    J.result[j] = results[j];
+    J.phi[j] = phi + 8 * p.first[j];
+  }
+  return J;
+}
+
+static int run_msm(const MsmJobs& J, const MsmPlan& p, char* ws, cudaStream_t s) {
   uint32_t* keys0 = reinterpret_cast<uint32_t*>(ws + p.off_keys0);
   uint32_t* keys1 = reinterpret_cast<uint32_t*>(ws + p.off_keys1);
   uint32_t* vals0 = reinterpret_cast<uint32_t*>(ws + p.off_vals0);
   uint32_t* vals1 = reinterpret_cast<uint32_t*>(ws + p.off_vals1);
   uint64_t* buckets = reinterpret_cast<uint64_t*>(ws + p.off_buckets);
-
-  uint64_t* phi = reinterpret_cast<uint64_t*>(ws + p.off_phi);
+  const int64_t windows = (int64_t)p.count * p.W;
 
   // 1. digits (GLV halves) and the phi images of the points
   {
     ProfSpan span("msm_digits", s);
-    k_msm_digits<<<grid_for(p.n, 256), 256, 0, s>>>(scalars, p.n, p.w, p.W, p.none, keys0, vals0);
+    k_msm_digits<<<grid_for(p.n, 256), 256, 0, s>>>(J, p.w, p.W, p.none, keys0, vals0);
     ZKB_TRY(check_launch("msm digits"));
-    k_msm_phi<<<grid_for(p.n, 256), 256, 0, s>>>(points, p.n, phi);
+    k_msm_phi<<<grid_for(p.n, 256), 256, 0, s>>>(J);
     ZKB_TRY(check_launch("msm phi points"));
   }
 
@@ -621,7 +728,7 @@ static int run_msm(const uint64_t* points, const uint64_t* scalars, const MsmPla
   const uint32_t* svals = vb.Current();
 
   // 3. buckets
-  const int64_t nbuckets = (int64_t)p.W * p.nb;
+  const int64_t nbuckets = windows * p.nb;
   k_xyzz_fill_identity<<<grid_for(nbuckets, 256), 256, 0, s>>>(buckets, nbuckets);
   ZKB_TRY(check_launch("msm bucket init"));
   uint32_t* sk[2] = {reinterpret_cast<uint32_t*>(ws + p.off_slot_keys_a),
@@ -631,8 +738,13 @@ static int run_msm(const uint64_t* points, const uint64_t* scalars, const MsmPla
   {
     ProfSpan span("msm_acc_points", s);
     const unsigned grid = (unsigned)((p.T1 + 127) / 128);
-    k_msm_acc_points<<<grid, 128, 0, s>>>(points, phi, p.n, skeys, svals, p.E, p.k1,
-                                          p.none, buckets, sk[0], sp[0]);
+    if (p.count > 1) {
+      k_msm_acc_points_batch<<<grid, 128, 0, s>>>(J, skeys, svals, p.E, p.k1, p.none, buckets,
+                                                  sk[0], sp[0]);
+    } else {
+      k_msm_acc_points<<<grid, 128, 0, s>>>(J, skeys, svals, p.E, p.k1, p.none, buckets, sk[0],
+                                            sp[0]);
+    }
     ZKB_TRY(check_launch("msm bucket accumulation"));
   }
   {
@@ -665,9 +777,9 @@ static int run_msm(const uint64_t* points, const uint64_t* scalars, const MsmPla
     const int64_t L = 1ll << p.log_l;
     while (G > L) {
       const int64_t G_out = G / L;
-      const int64_t threads = (int64_t)p.W * G_out;
+      const int64_t threads = windows * G_out;
       k_msm_reduce<<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(X, U, G, p.log_l, delta,
-                                                                     p.W, rs[r], ru[r], 0);
+                                                                     (int)windows, rs[r], ru[r], 0);
       ZKB_TRY(check_launch("msm window reduction"));
       X = rs[r];
       U = ru[r];
@@ -675,15 +787,99 @@ static int run_msm(const uint64_t* points, const uint64_t* scalars, const MsmPla
       G = G_out;
       delta = 0;
     }
-    k_msm_reduce<<<(unsigned)((p.W + 127) / 128), 128, 0, s>>>(X, U, G, p.log_l, delta, p.W,
-                                                               nullptr, wsum, 1);
+    k_msm_reduce<<<(unsigned)((windows + 127) / 128), 128, 0, s>>>(X, U, G, p.log_l, delta,
+                                                                   (int)windows, nullptr, wsum, 1);
     ZKB_TRY(check_launch("msm window sums"));
   }
 
   // 5. finalize
   ProfSpan fin_span("msm_finalize", s);
-  k_msm_finalize<<<1, 1, 0, s>>>(wsum, p.W, p.w, result);
+  k_msm_finalize<<<1, p.count < 32 ? 32 : p.count, 0, s>>>(J, wsum, p.W, p.w);
   return check_launch("msm finalize");
+}
+
+// ---- batches of jobs --------------------------------------------------------
+
+// Jobs with the same window share one pipeline run (a chunk), at most
+// kMsmMaxBatch jobs and 2^31 sorted pairs per chunk; chunks run concurrently
+// on side streams, each in its own slice of the workspace.
+struct MsmChunk {
+  int w = 0;
+  std::vector<int> jobs;  // indices into the caller's job array
+  MsmPlan plan;
+  size_t offset = 0;
+};
+
+static int validate_job(const zkb_msm_job& j, int index) {
+  if (j.n < 0) return fail(ZKB_EINVAL, "job %d: negative point count", index);
+  if (j.n >= (1ll << 30)) return fail(ZKB_EINVAL, "job %d: at most 2^30 - 1 points per MSM", index);
+  if (j.window_size < 0 || j.window_size > kMsmMaxWindow) {
+    return fail(ZKB_EINVAL, "job %d: window_size must be in 1..%d (or 0 for the default), got %d",
+                index, kMsmMaxWindow, j.window_size);
+  }
+  if (!j.result) return fail(ZKB_EINVAL, "job %d: null result buffer", index);
+  ZKB_TRY(check_align(j.result, 8, "result"));
+  if (j.n == 0) return ZKB_OK;
+  if (!j.points || !j.scalars) return fail(ZKB_EINVAL, "job %d: null buffer", index);
+  ZKB_TRY(check_align(j.points, 16, "points"));
+  ZKB_TRY(check_align(j.scalars, 16, "scalars"));
+  return ZKB_OK;
+}
+
+static int plan_batch(const zkb_msm_job* jobs, int count, std::vector<MsmChunk>& chunks,
+                      size_t& total) {
+  chunks.clear();
+  total = 0;
+  if (count < 0) return fail(ZKB_EINVAL, "negative job count");
+  if (count > 0 && !jobs) return fail(ZKB_EINVAL, "null job array");
+  std::vector<int> order;
+  for (int i = 0; i < count; ++i) {
+    ZKB_TRY(validate_job(jobs[i], i));
+    if (jobs[i].n > 0) order.push_back(i);
+  }
+  auto window_of = [&](int i) {
+    return jobs[i].window_size ? jobs[i].window_size : default_window(jobs[i].n);
+  };
+  // by window, then by size (largest first) so each chunk's sort stays in range
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    const int wa = window_of(a), wb = window_of(b);
+    return wa != wb ? wa < wb : jobs[a].n > jobs[b].n;
+  });
+  for (int i : order) {
+    const int w = window_of(i);
+    const int64_t pairs = 2 * (int64_t)num_windows(w) * jobs[i].n;
+    if (pairs >= (1ll << 31)) {
+      return fail(ZKB_EINVAL, "%lld points at window %d exceed the sort's 2^31 pairs",
+                  (long long)jobs[i].n, w);
+    }
+    bool fits = !chunks.empty() && chunks.back().w == w &&
+                (int)chunks.back().jobs.size() < kMsmMaxBatch;
+    if (fits) {
+      int64_t cur = 0;
+      for (int k : chunks.back().jobs) cur += 2 * (int64_t)num_windows(w) * jobs[k].n;
+      fits = cur + pairs < (1ll << 31);
+    }
+    if (!fits) {
+      chunks.emplace_back();
+      chunks.back().w = w;
+    }
+    chunks.back().jobs.push_back(i);
+  }
+  for (auto& c : chunks) {
+    std::vector<int64_t> sizes;
+    for (int k : c.jobs) sizes.push_back(jobs[k].n);
+    ZKB_TRY(make_plan(sizes.data(), (int)sizes.size(), c.w, c.plan));
+    c.offset = total;
+    total += align256(c.plan.total);
+  }
+  return ZKB_OK;
+}
+
+// One MSM through the batch pipeline.
+static int run_single(const uint64_t* points, const uint64_t* scalars, uint64_t* result,
+                      const MsmPlan& p, char* ws, cudaStream_t s) {
+  const MsmJobs J = job_table(p, &points, &scalars, &result, ws);
+  return run_msm(J, p, ws, s);
 }
 
 }  // namespace zkb
@@ -700,7 +896,7 @@ size_t zkb_msm_workspace_bytes(int64_t n, int window_size) {
   const int w = window_size ? window_size : default_window(n);
   if (w < 1 || w > kMsmMaxWindow) return 0;
   MsmPlan p;
-  if (make_plan(n, w, p) != ZKB_OK) return 0;
+  if (make_plan(&n, 1, w, p) != ZKB_OK) return 0;
   return p.total;
 }
 
@@ -726,7 +922,7 @@ int zkb_msm(const uint64_t* points, const uint64_t* scalars, int64_t n, int wind
   ZKB_TRY(check_align(workspace, 256, "workspace"));
   const int w = window_size ? window_size : default_window(n);
   MsmPlan p;
-  ZKB_TRY(make_plan(n, w, p));
+  ZKB_TRY(make_plan(&n, 1, w, p));
   if ((int64_t)p.E >= (1ll << 31)) {
     return fail(ZKB_EINVAL, "%lld points at window %d exceed the sort's 2^31 pairs",
                 (long long)n, w);
@@ -735,7 +931,62 @@ int zkb_msm(const uint64_t* points, const uint64_t* scalars, int64_t n, int wind
     return fail(ZKB_EWORKSPACE, "MSM of %lld points at window %d needs %zu workspace bytes, got %zu",
                 (long long)n, w, p.total, workspace_bytes);
   }
-  return run_msm(points, scalars, p, result, reinterpret_cast<char*>(workspace), s);
+  return run_single(points, scalars, result, p, reinterpret_cast<char*>(workspace), s);
+}
+
+size_t zkb_msm_batch_workspace_bytes(const zkb_msm_job* jobs, int count) {
+  set_error("%s", "");
+  std::vector<MsmChunk> chunks;
+  size_t total = 0;
+  if (plan_batch(jobs, count, chunks, total) != ZKB_OK) return 0;
+  return total;
+}
+
+int zkb_msm_batch(const zkb_msm_job* jobs, int count, void* workspace, size_t workspace_bytes,
+                  void* stream) {
+  set_error("%s", "");
+  std::vector<MsmChunk> chunks;
+  size_t total = 0;
+  ZKB_TRY(plan_batch(jobs, count, chunks, total));
+  if (total > 0) {
+    ZKB_TRY(check_align(workspace, 256, "workspace"));
+    if (!workspace || workspace_bytes < total) {
+      return fail(ZKB_EWORKSPACE, "MSM batch of %d jobs needs %zu workspace bytes, got %zu", count,
+                  total, workspace_bytes);
+    }
+  }
+  cudaStream_t s = as_stream(stream);
+  for (int i = 0; i < count; ++i) {
+    if (jobs[i].n == 0) {
+      k_msm_identity_result<<<1, 1, 0, s>>>(jobs[i].result);
+      ZKB_TRY(check_launch("msm identity"));
+    }
+  }
+  auto run_chunk = [&](const MsmChunk& c, cudaStream_t cs) {
+    std::vector<const uint64_t*> pts, scs;
+    std::vector<uint64_t*> res;
+    for (int k : c.jobs) {
+      pts.push_back(jobs[k].points);
+      scs.push_back(jobs[k].scalars);
+      res.push_back(jobs[k].result);
+    }
+    char* ws = reinterpret_cast<char*>(workspace) + c.offset;
+    const MsmJobs J = job_table(c.plan, pts.data(), scs.data(), res.data(), ws);
+    return run_msm(J, c.plan, ws, cs);
+  };
+  if (chunks.size() == 1) return run_chunk(chunks[0], s);
+  if (chunks.empty()) return ZKB_OK;
+  Fanout fan;
+  const int sides = (int)std::min<size_t>(chunks.size(), Fanout::kMaxSides);
+  ZKB_TRY(fan.fork(s, sides));
+  for (size_t c = 0; c < chunks.size(); ++c) {
+    const int rc = run_chunk(chunks[c], fan.side((int)c));
+    if (rc != ZKB_OK) {
+      fan.join(s);
+      return rc;
+    }
+  }
+  return fan.join(s);
 }
 
 }  // extern "C"
@@ -815,7 +1066,7 @@ int zkb_msm_no_alloc(const uint64_t* points, const uint64_t* scalars, int64_t n,
   ZKB_TRY(check_align(scalars, 16, "scalars"));
   const int w = window_size ? window_size : default_window(n);
   MsmPlan p;
-  ZKB_TRY(make_plan(n, w, p));
+  ZKB_TRY(make_plan(&n, 1, w, p));
   if (p.total > kNoAllocScratchBytes) {
     return fail(ZKB_EWORKSPACE,
                 "MSM of %lld points at window %d needs %zu bytes of scratch; the library's fixed "
@@ -824,7 +1075,7 @@ int zkb_msm_no_alloc(const uint64_t* points, const uint64_t* scalars, int64_t n,
   }
   void* scratch = nullptr;
   ZKB_TRY(static_scratch_address(&scratch));
-  return run_msm(points, scalars, p, result, reinterpret_cast<char*>(scratch), s);
+  return run_single(points, scalars, result, p, reinterpret_cast<char*>(scratch), s);
 }
 
 }  // extern "C"

@@ -18,10 +18,11 @@
 // stages there (one Montgomery multiplication per butterfly), and applies the
 // pass twiddle (and, for the first/last pass, the coset or n^-1 scaling) on
 // the way out: one HBM read and one HBM write per element per pass.
-#include <mutex>
-#include <list>
-#include <vector>
+#include <algorithm>
 #include <cstring>
+#include <list>
+#include <mutex>
+#include <vector>
 
 #include "field_host.h"
 #include "profile.h"
@@ -176,7 +177,9 @@ static std::mutex g_ntt_mutex;
 static std::list<RootEntry> g_roots;    // most recently used first
 static std::list<ScaleEntry> g_scales;  // most recently used first
 static constexpr size_t kMaxRootEntries = 16;  // like the reference's lru_cache(16)
-static constexpr size_t kMaxScaleEntries = 64;
+// At least the 64 transforms of one batch, whose tables must all stay alive
+// until its launch (an entry used in the batch is never the least recent).
+static constexpr size_t kMaxScaleEntries = 96;
 
 template <class F>
 static int build_roots(const F& f, const TableKey& key, RootTables& t, void** mem,
@@ -281,16 +284,17 @@ __device__ __forceinline__ void root_power(uint32_t r[8], const NttPass& a, uint
   fe_mul(r, lo, hi, f);
 }
 
-template <class F>
-__global__ void __launch_bounds__(kNttThreads, 1) k_ntt_pass(F f, NttPass a) {
-  extern __shared__ uint4 smem_raw[];
-  uint64_t* sm = reinterpret_cast<uint64_t*>(smem_raw);
+// One tile (CTA-sized piece) `bid` of pass a. kFresh: the pass reads rows
+// that other CTAs wrote earlier in the same kernel (the batched form), so its
+// row loads bypass L1.
+template <class F, bool kFresh>
+__device__ __forceinline__ void ntt_tile(const F& f, const NttPass& a, int64_t bid,
+                                         uint64_t* sm) {
   const int lr = a.lr, lc = a.lc;
   const int R = 1 << lr, C = 1 << lc;
   const int total = C << lr;
   const int64_t S = 1ll << a.ls;
   const int64_t B = (int64_t)R << a.ls;
-  const int64_t bid = blockIdx.x;
 
   // Column bases.
   //   non-last: o = bid / (S / C), first inner index j0 = (bid % (S / C)) * C,
@@ -332,7 +336,11 @@ __global__ void __launch_bounds__(kNttThreads, 1) k_ntt_pass(F f, NttPass a) {
     const int64_t pos = !a.last ? o * B + (int64_t)j * S + j0 + c
                                 : (((k1_0 + c) << a.lR2) + k2) * R + j;
     uint32_t x[8];
-    fe_load_nc(x, a.in + 4 * pos);
+    if (kFresh && !a.first) {
+      fe_load_cg(x, a.in + 4 * pos);
+    } else {
+      fe_load_nc(x, a.in + 4 * pos);
+    }
     if (a.first && a.g_lo && !a.inverse) {
       const uint64_t m = (1ull << a.gs) - 1;
       uint32_t lo[8], hi[8];
@@ -455,6 +463,87 @@ __global__ void __launch_bounds__(kNttThreads, 1) k_ntt_pass(F f, NttPass a) {
   }
 }
 
+template <class F>
+__global__ void __launch_bounds__(kNttThreads, 1) k_ntt_pass(F f, NttPass a) {
+  extern __shared__ uint4 smem_raw[];
+  ntt_tile<F, false>(f, a, blockIdx.x, reinterpret_cast<uint64_t*>(smem_raw));
+}
+
+// ---------------------------------------------------------------------------
+// Batched form: one persistent launch for many transforms
+// ---------------------------------------------------------------------------
+//
+// Every pass of every transform in the batch is a list of tiles; the tiles
+// are numbered pass by pass, all first passes before all second passes (and
+// those before all third passes). CTAs take tile numbers from a device
+// counter in that order. A tile of pass q > 0 may start only when every tile
+// of pass q - 1 of its transform has finished: thread 0 waits on that pass's
+// completion counter. The tiles it waits for carry smaller numbers, so they
+// were taken earlier by CTAs that are already running and that wait, if at
+// all, only on still smaller numbers: the waits always end. Each wait is
+// still bounded (about a second); a CTA that gives up sets the status word
+// to ZKB_ETIMEOUT and stops taking tiles.
+
+static constexpr int kMaxBatchPasses = 192;  // 64 transforms x 3 passes
+static constexpr int kBatchThreads = 256;
+static constexpr unsigned kBatchSpinLimit = 1u << 22;  // x >= 256 ns each
+
+struct NttBatchTable {
+  int num_passes;
+  int64_t tile_start[kMaxBatchPasses + 1];  // first tile number of each pass
+  int dep[kMaxBatchPasses];                 // pass that must finish first, or -1
+  NttPass pass[kMaxBatchPasses];
+};
+
+template <class F>
+__global__ void __launch_bounds__(kBatchThreads) k_ntt_batch(F f, const __grid_constant__ NttBatchTable T,
+                                                             unsigned long long* next_tile,
+                                                             unsigned* done, int* status) {
+  extern __shared__ uint4 smem_raw[];
+  uint64_t* sm = reinterpret_cast<uint64_t*>(smem_raw);
+  __shared__ long long s_tile;
+  __shared__ int s_pass, s_go;
+  const long long total = T.tile_start[T.num_passes];
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const long long tile = (long long)atomicAdd(next_tile, 1ull);
+      int p = 0, go = tile < total && *(volatile int*)status == 0;
+      if (go) {
+        int lo = 0, hi = T.num_passes - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (T.tile_start[mid] <= tile) lo = mid; else hi = mid - 1;
+        }
+        p = lo;
+        const int d = T.dep[p];
+        if (d >= 0) {
+          const unsigned need = (unsigned)(T.tile_start[d + 1] - T.tile_start[d]);
+          unsigned spins = 0;
+          while (*(volatile unsigned*)(done + d) < need) {
+            if (++spins > kBatchSpinLimit) {
+              atomicExch(status, ZKB_ETIMEOUT);
+              go = 0;
+              break;
+            }
+            __nanosleep(256);
+          }
+          __threadfence();
+        }
+      }
+      s_tile = tile;
+      s_pass = p;
+      s_go = go;
+    }
+    __syncthreads();
+    if (!s_go) break;
+    const int p = s_pass;
+    ntt_tile<F, true>(f, T.pass[p], s_tile - T.tile_start[p], sm);
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) atomicAdd(done + p, 1u);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
@@ -491,11 +580,70 @@ size_t workspace_bytes(int64_t n) {
   return (size_t)n * 32;
 }
 
+// Cached tables for a transform of n = 2^log_n rows: the root tables of `key`
+// and, for an inverse or coset transform, its scaling tables.
 template <class F>
-static int run_ntt(const F& f, const zkb_field* field, const uint64_t* in, uint64_t* out,
-                   int64_t n, int invert, const uint64_t* omega, const uint64_t* coset,
-                   void* workspace, size_t ws_bytes, cudaStream_t s) {
-  const int log_n = ilog2(n);
+static int lookup_tables(const F& f, const TableKey& key, int64_t n, int log_n, int invert,
+                         const uint64_t* coset, RootTables& rt, ScaleTables& st, cudaStream_t s) {
+  std::lock_guard<std::mutex> lock(g_ntt_mutex);
+  auto it = g_roots.begin();
+  for (; it != g_roots.end(); ++it)
+    if (it->key == key) break;
+  if (it == g_roots.end()) {
+    RootEntry e;
+    e.key = key;
+    e.mem = nullptr;
+    int rc = build_roots(f, key, e.t, &e.mem, s);
+    if (rc != ZKB_OK) {
+      if (e.mem) cudaFree(e.mem);
+      return rc;
+    }
+    g_roots.push_front(e);
+    if (g_roots.size() > kMaxRootEntries) {
+      // kernels queued on any stream may still read the evicted tables
+      cudaDeviceSynchronize();
+      cudaFree(g_roots.back().mem);
+      g_roots.pop_back();
+    }
+  } else {
+    g_roots.splice(g_roots.begin(), g_roots, it);
+  }
+  rt = g_roots.front().t;
+  st = ScaleTables();
+  if (!invert && !coset) return ZKB_OK;
+  ScaleKey sk;
+  sk.root = key;
+  std::memset(sk.g, 0, sizeof sk.g);
+  if (coset) std::memcpy(sk.g, coset, sizeof sk.g);
+  sk.has_coset = coset != nullptr;
+  sk.inverse = invert;
+  sk.n = n;
+  auto jt = g_scales.begin();
+  for (; jt != g_scales.end(); ++jt)
+    if (jt->key == sk) break;
+  if (jt == g_scales.end()) {
+    ScaleEntry e;
+    e.key = sk;
+    e.mem = nullptr;
+    int rc = build_scale(f, sk, log_n, e.t, &e.mem, s);
+    if (rc != ZKB_OK) {
+      if (e.mem) cudaFree(e.mem);
+      return rc;
+    }
+    g_scales.push_front(e);
+    if (g_scales.size() > kMaxScaleEntries) {
+      cudaDeviceSynchronize();
+      cudaFree(g_scales.back().mem);
+      g_scales.pop_back();
+    }
+  } else {
+    g_scales.splice(g_scales.begin(), g_scales, jt);
+  }
+  st = g_scales.front().t;
+  return ZKB_OK;
+}
+
+static TableKey table_key(const zkb_field* field, const uint64_t* omega, int log_n, int device) {
   TableKey key;
   std::memcpy(key.modulus, field->modulus, sizeof key.modulus);
   if (omega) {
@@ -505,80 +653,40 @@ static int run_ntt(const F& f, const zkb_field* field, const uint64_t* in, uint6
     std::memcpy(key.omega, kFrRoot28, sizeof key.omega);
     key.log_N = kMaxLogN;
   }
-  ZKB_TRY(check_cuda(cudaGetDevice(&key.device), "cudaGetDevice"));
+  key.device = device;
+  return key;
+}
 
-  RootTables rt;
-  ScaleTables st;
-  {
-    std::lock_guard<std::mutex> lock(g_ntt_mutex);
-    auto it = g_roots.begin();
-    for (; it != g_roots.end(); ++it)
-      if (it->key == key) break;
-    if (it == g_roots.end()) {
-      RootEntry e;
-      e.key = key;
-      e.mem = nullptr;
-      int rc = build_roots(f, key, e.t, &e.mem, s);
-      if (rc != ZKB_OK) {
-        if (e.mem) cudaFree(e.mem);
-        return rc;
-      }
-      g_roots.push_front(e);
-      if (g_roots.size() > kMaxRootEntries) {
-        // kernels queued on any stream may still read the evicted tables
-        cudaDeviceSynchronize();
-        cudaFree(g_roots.back().mem);
-        g_roots.pop_back();
-      }
-    } else {
-      g_roots.splice(g_roots.begin(), g_roots, it);
-    }
-    rt = g_roots.front().t;
+// One launch of the pass kernel: its parameters and shape.
+struct PassLaunch {
+  NttPass a;
+  int64_t ctas;
+  int threads;
+  size_t smem;
+};
 
-    if (invert || coset) {
-      ScaleKey sk;
-      sk.root = key;
-      std::memset(sk.g, 0, sizeof sk.g);
-      if (coset) std::memcpy(sk.g, coset, sizeof sk.g);
-      sk.has_coset = coset != nullptr;
-      sk.inverse = invert;
-      sk.n = n;
-      auto jt = g_scales.begin();
-      for (; jt != g_scales.end(); ++jt)
-        if (jt->key == sk) break;
-      if (jt == g_scales.end()) {
-        ScaleEntry e;
-        e.key = sk;
-        e.mem = nullptr;
-        int rc = build_scale(f, sk, log_n, e.t, &e.mem, s);
-        if (rc != ZKB_OK) {
-          if (e.mem) cudaFree(e.mem);
-          return rc;
-        }
-        g_scales.push_front(e);
-        if (g_scales.size() > kMaxScaleEntries) {
-          cudaDeviceSynchronize();
-          cudaFree(g_scales.back().mem);
-          g_scales.pop_back();
-        }
-      } else {
-        g_scales.splice(g_scales.begin(), g_scales, jt);
-      }
-      st = g_scales.front().t;
-    }
-  }
-
+// The passes of one transform. cta_log / threads: the tile and block size,
+// or 0 for the size-based choice (and the "ntt.cta_log_elems" / "ntt.threads"
+// knobs, which override it).
+static void plan_passes(int64_t n, int log_n, int invert, const RootTables& rt,
+                        const ScaleTables& st, const uint64_t* in, uint64_t* out, uint64_t* tmp,
+                        int sms, int cta_log, int threads, std::vector<PassLaunch>& passes) {
   const std::vector<int> radices = plan_radices(log_n);
   const int P = (int)radices.size();
-  uint64_t* tmp = P > 1 ? reinterpret_cast<uint64_t*>(workspace) : nullptr;
-  if (P > 1 && (!workspace || ws_bytes < workspace_bytes(n))) {
-    return fail(ZKB_EWORKSPACE, "NTT of %lld rows needs %zu workspace bytes, got %zu",
-                (long long)n, workspace_bytes(n), ws_bytes);
+  // columns per CTA: the tile C R is at most 2^cta_log elements. Auto:
+  // 4096-row tiles of 512 threads (one CTA per SM, 128 KiB of shared memory)
+  // when that gives at least 16 CTAs per SM (2^24 rows and up on a B200),
+  // else 1024-row tiles of 256 threads, several per SM, which measured faster
+  // from 2^12 to 2^22 rows.
+  if (cta_log == 0) {
+    cta_log = tune_get("ntt.cta_log_elems");
+    if (cta_log < 9) cta_log = (n >> kMaxLogR) >= 16 * sms ? kMaxLogR : 10;
   }
-
-  int sms = 0;
-  ZKB_TRY(check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, key.device),
-                     "SM count"));
+  if (threads == 0) {
+    threads = tune_get("ntt.threads");
+    if (threads < 64) threads = cta_log >= kMaxLogR ? 512 : 256;
+  }
+  passes.clear();
   int ls = log_n;  // stride exponent of the current pass: S_q = 2^(log_n - sum of radices so far)
   for (int q = 0; q < P; ++q) {
     NttPass a;
@@ -602,44 +710,197 @@ static int run_ntt(const F& f, const zkb_field* field, const uint64_t* in, uint6
     a.g_hi = st.g_hi;
     a.gs = st.gs;
     a.scale = st.scale;
-    // columns per CTA: the tile C R is at most 2^"ntt.cta_log_elems" elements.
-    // Auto (0): 4096-row tiles of 512 threads (one CTA per SM, 128 KiB of
-    // shared memory) when that gives at least 16 CTAs per SM (2^24 rows and
-    // up on a B200), else 1024-row tiles of 256 threads, several per SM,
-    // which measured faster from 2^12 to 2^22 rows.
-    int cta_log = tune_get("ntt.cta_log_elems");
-    int threads = tune_get("ntt.threads");
-    if (cta_log < 9) cta_log = (n >> kMaxLogR) >= 16 * sms ? kMaxLogR : 10;
-    if (threads < 64) threads = cta_log >= kMaxLogR ? 512 : 256;
     int lc = cta_log > a.lr ? cta_log - a.lr : 0;
-    int64_t ctas;
     if (!a.last) {
       if (lc > a.ls) lc = a.ls;
-      ctas = n >> (a.lr + lc);
     } else {
       // R1 = first radix, R2 = the middle radix (P <= 3)
-      const int lR1 = radices[0];
-      const int lR2 = P >= 3 ? radices[1] : 0;
-      a.lR1 = P >= 2 ? lR1 : 0;
-      a.lR2 = lR2;
-      const int k1_bits = P >= 2 ? lR1 : 0;
-      if (lc > k1_bits) lc = k1_bits;
-      ctas = n >> (a.lr + lc);
+      a.lR1 = P >= 2 ? radices[0] : 0;
+      a.lR2 = P >= 3 ? radices[1] : 0;
+      if (lc > a.lR1) lc = a.lR1;
     }
     a.lc = lc;
+    PassLaunch L;
+    L.a = a;
+    L.ctas = n >> (a.lr + lc);
     // padded columns, then the stage table (R / 2 rows)
-    const size_t smem = (size_t)(1 << lc) * ((32u << a.lr) + 16) + ((size_t)16 << a.lr);
+    L.smem = (size_t)(1 << lc) * ((32u << a.lr) + 16) + ((size_t)16 << a.lr);
+    const int half_total = (1 << (a.lr + lc)) >> 1;
+    L.threads = threads;
+    if (half_total < L.threads) L.threads = half_total < 32 ? 32 : half_total;
+    passes.push_back(L);
+  }
+}
+
+static int sm_count(int device, int* sms) {
+  return check_cuda(cudaDeviceGetAttribute(sms, cudaDevAttrMultiProcessorCount, device),
+                    "SM count");
+}
+
+template <class F>
+static int run_ntt(const F& f, const zkb_field* field, const uint64_t* in, uint64_t* out,
+                   int64_t n, int invert, const uint64_t* omega, const uint64_t* coset,
+                   void* workspace, size_t ws_bytes, cudaStream_t s) {
+  const int log_n = ilog2(n);
+  int device = 0;
+  ZKB_TRY(check_cuda(cudaGetDevice(&device), "cudaGetDevice"));
+  const TableKey key = table_key(field, omega, log_n, device);
+  RootTables rt;
+  ScaleTables st;
+  ZKB_TRY(lookup_tables(f, key, n, log_n, invert, coset, rt, st, s));
+
+  const size_t need = workspace_bytes(n);
+  if (need && (!workspace || ws_bytes < need)) {
+    return fail(ZKB_EWORKSPACE, "NTT of %lld rows needs %zu workspace bytes, got %zu",
+                (long long)n, need, ws_bytes);
+  }
+  int sms = 0;
+  ZKB_TRY(sm_count(device, &sms));
+  std::vector<PassLaunch> passes;
+  plan_passes(n, log_n, invert, rt, st, in, out, reinterpret_cast<uint64_t*>(workspace), sms, 0,
+              0, passes);
+  const int P = (int)passes.size();
+  for (int q = 0; q < P; ++q) {
+    const PassLaunch& L = passes[q];
     auto kern = k_ntt_pass<F>;
     ZKB_TRY(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)smem),
+                                            (int)L.smem),
                        "NTT shared memory attribute"));
-    const int half_total = (1 << (a.lr + lc)) >> 1;
-    if (half_total < threads) threads = half_total < 32 ? 32 : half_total;
-    {
-      ProfSpan span(a.last ? (q == 0 ? "ntt_single_pass" : "ntt_last_pass") : "ntt_column_pass", s);
-      kern<<<(unsigned)ctas, threads, smem, s>>>(f, a);
-      ZKB_TRY(check_launch("NTT pass launch"));
+    ProfSpan span(L.a.last ? (q == 0 ? "ntt_single_pass" : "ntt_last_pass") : "ntt_column_pass", s);
+    kern<<<(unsigned)L.ctas, L.threads, L.smem, s>>>(f, L.a);
+    ZKB_TRY(check_launch("NTT pass launch"));
+  }
+  return ZKB_OK;
+}
+
+// ---- batches ----------------------------------------------------------------
+
+static constexpr int kMaxBatchJobs = 64;
+
+// Workspace of a batch: the tile counter and status word, one completion
+// counter per pass, then each multi-pass transform's intermediate rows.
+struct BatchLayout {
+  size_t off_counters = 0;  // next tile (u64), status (i32)
+  size_t off_done = 0;      // u32 per pass
+  std::vector<size_t> off_tmp;
+  size_t total = 0;
+};
+
+static int batch_layout(const zkb_ntt_job* jobs, int count, BatchLayout& L) {
+  if (count < 0 || count > kMaxBatchJobs) {
+    return fail(ZKB_EINVAL, "an NTT batch holds 0..%d transforms, got %d", kMaxBatchJobs, count);
+  }
+  if (count > 0 && !jobs) return fail(ZKB_EINVAL, "null job array");
+  L.off_tmp.assign(count, 0);
+  size_t off = 0;
+  L.off_counters = off;
+  off += 256;
+  L.off_done = off;
+  off += (size_t)kMaxBatchPasses * 4;
+  off = (off + 255) & ~(size_t)255;
+  for (int j = 0; j < count; ++j) {
+    const int64_t n = jobs[j].n;
+    if (n < 0 || (n & (n - 1)) || n > (1ll << kMaxLogN)) {
+      return fail(ZKB_EINVAL, "job %d: NTT length must be a power of 2 up to 2^28, got %lld", j,
+                  (long long)n);
     }
+    const size_t need = workspace_bytes(n);
+    L.off_tmp[j] = off;
+    off += (need + 255) & ~(size_t)255;
+  }
+  L.total = off;
+  return ZKB_OK;
+}
+
+template <class F>
+static int run_ntt_batch(const F& f, const zkb_field* field, const zkb_ntt_job* jobs, int count,
+                         char* ws, const BatchLayout& L, int32_t* status_out, cudaStream_t s) {
+  int device = 0;
+  ZKB_TRY(check_cuda(cudaGetDevice(&device), "cudaGetDevice"));
+  int sms = 0;
+  ZKB_TRY(sm_count(device, &sms));
+  // largest transforms first, so that their long passes start early
+  std::vector<int> order;
+  for (int j = 0; j < count; ++j)
+    if (jobs[j].n > 1) order.push_back(j);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return jobs[a].n > jobs[b].n; });
+
+  static NttBatchTable T;  // 26 KB: built under the table mutex below, copied into the launch
+  static std::mutex table_mutex;
+  std::lock_guard<std::mutex> tlock(table_mutex);
+  std::memset(&T, 0, sizeof T);
+  // tables (built on first use; at most 64 scaling tables, which the cache holds)
+  std::vector<RootTables> rts(order.size());
+  std::vector<ScaleTables> sts(order.size());
+  int max_lr = 0;
+  for (size_t k = 0; k < order.size(); ++k) {
+    const zkb_ntt_job& J = jobs[order[k]];
+    const int log_n = ilog2(J.n);
+    ZKB_TRY(lookup_tables(f, table_key(field, nullptr, log_n, device), J.n, log_n, J.invert,
+                          J.has_coset ? J.coset : nullptr, rts[k], sts[k], s));
+    for (int r : plan_radices(log_n)) max_lr = std::max(max_lr, r);
+  }
+  // one tile shape for every pass: 2^max(10, largest radix) rows, 256 threads
+  const int cta_log = std::max(10, max_lr);
+  std::vector<std::vector<PassLaunch>> plans(order.size());
+  for (size_t k = 0; k < order.size(); ++k) {
+    const zkb_ntt_job& J = jobs[order[k]];
+    plan_passes(J.n, ilog2(J.n), J.invert, rts[k], sts[k], J.in, J.out,
+                reinterpret_cast<uint64_t*>(ws + L.off_tmp[order[k]]), sms, cta_log,
+                kBatchThreads, plans[k]);
+  }
+  // tile numbering: pass q of every transform before pass q + 1 of any
+  size_t smem = 0;
+  int np = 0;
+  int64_t tiles = 0;
+  std::vector<int> pass_index(order.size() * 3, -1);
+  for (int q = 0; q < 3; ++q) {
+    for (size_t k = 0; k < order.size(); ++k) {
+      if (q >= (int)plans[k].size()) continue;
+      if (np >= kMaxBatchPasses) return fail(ZKB_EINVAL, "NTT batch has too many passes");
+      const PassLaunch& P = plans[k][q];
+      T.pass[np] = P.a;
+      T.dep[np] = q > 0 ? pass_index[k * 3 + q - 1] : -1;
+      T.tile_start[np] = tiles;
+      pass_index[k * 3 + q] = np;
+      tiles += P.ctas;
+      smem = std::max(smem, P.smem);
+      ++np;
+    }
+  }
+  T.num_passes = np;
+  T.tile_start[np] = tiles;
+
+  // n = 1 transforms are copies
+  for (int j = 0; j < count; ++j) {
+    if (jobs[j].n == 1) {
+      ZKB_TRY(check_cuda(cudaMemcpyAsync(jobs[j].out, jobs[j].in, 32, cudaMemcpyDeviceToDevice, s),
+                         "NTT copy"));
+    }
+  }
+  unsigned long long* next_tile = reinterpret_cast<unsigned long long*>(ws + L.off_counters);
+  int* status = reinterpret_cast<int*>(ws + L.off_counters + 8);
+  unsigned* done = reinterpret_cast<unsigned*>(ws + L.off_done);
+  ZKB_TRY(check_cuda(cudaMemsetAsync(ws, 0, L.off_done + (size_t)kMaxBatchPasses * 4, s),
+                     "NTT batch counters"));
+  if (np > 0) {
+    auto kern = k_ntt_batch<F>;
+    ZKB_TRY(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)smem),
+                       "NTT batch shared memory attribute"));
+    int per_sm = 0;
+    ZKB_TRY(check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBatchThreads,
+                                                                     smem),
+                       "NTT batch occupancy"));
+    if (per_sm < 1) per_sm = 1;
+    const int64_t grid = std::min<int64_t>(tiles, (int64_t)sms * per_sm);
+    ProfSpan span("ntt_batch", s);
+    kern<<<(unsigned)grid, kBatchThreads, smem, s>>>(f, T, next_tile, done, status);
+    ZKB_TRY(check_launch("NTT batch launch"));
+  }
+  if (status_out) {
+    ZKB_TRY(check_cuda(cudaMemcpyAsync(status_out, status, 4, cudaMemcpyDeviceToDevice, s),
+                       "NTT batch status"));
   }
   return ZKB_OK;
 }
@@ -677,6 +938,40 @@ int zkb_ntt(const zkb_field* f, const uint64_t* in, uint64_t* out, int64_t n, in
   return with_field(f, [&](auto fp) {
     return run_ntt(fp, f, in, out, n, invert, omega, coset, workspace, workspace_bytes, s);
   });
+}
+
+size_t zkb_ntt_batch_workspace_bytes(const zkb_ntt_job* jobs, int count) {
+  set_error("%s", "");
+  BatchLayout L;
+  if (batch_layout(jobs, count, L) != ZKB_OK) return 0;
+  return L.total;
+}
+
+int zkb_ntt_batch(const zkb_field* f, const zkb_ntt_job* jobs, int count, void* workspace,
+                  size_t workspace_bytes, int32_t* status, void* stream) {
+  set_error("%s", "");
+  ZKB_TRY(check_field(f));
+  if (f->kind != ZKB_FIELD_BN254_FR) {
+    return fail(ZKB_EINVAL, "batched NTTs use BN254 Fr's built-in roots of unity");
+  }
+  BatchLayout L;
+  ZKB_TRY(batch_layout(jobs, count, L));
+  if (!workspace || workspace_bytes < L.total) {
+    return fail(ZKB_EWORKSPACE, "NTT batch of %d transforms needs %zu workspace bytes, got %zu",
+                count, L.total, workspace_bytes);
+  }
+  ZKB_TRY(check_align(workspace, 256, "workspace"));
+  if (status) ZKB_TRY(check_align(status, 4, "status"));
+  for (int j = 0; j < count; ++j) {
+    const zkb_ntt_job& J = jobs[j];
+    if (J.n == 0) continue;
+    if (!J.in || !J.out) return fail(ZKB_EINVAL, "job %d: null buffer", j);
+    if (J.in == J.out) return fail(ZKB_EINVAL, "job %d: NTT output must not alias its input", j);
+    ZKB_TRY(check_align(J.in, 16, "in"));
+    ZKB_TRY(check_align(J.out, 16, "out"));
+  }
+  cudaStream_t s = as_stream(stream);
+  return run_ntt_batch(FrP{}, f, jobs, count, reinterpret_cast<char*>(workspace), L, status, s);
 }
 
 }  // extern "C"

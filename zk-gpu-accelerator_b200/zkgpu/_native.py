@@ -47,10 +47,38 @@ class ZkbField(ctypes.Structure):
     ]
 
 
+class ZkbMsmJob(ctypes.Structure):
+    """zkb_msm_job from include/zkb200.h: one MSM of a batch (device pointers)."""
+
+    _fields_ = [
+        ("points", ctypes.c_void_p),
+        ("scalars", ctypes.c_void_p),
+        ("n", ctypes.c_int64),
+        ("result", ctypes.c_void_p),
+        ("window_size", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+    ]
+
+
+class ZkbNttJob(ctypes.Structure):
+    """zkb_ntt_job from include/zkb200.h: one transform of a batch (device pointers)."""
+
+    _fields_ = [
+        ("input", ctypes.c_void_p),
+        ("out", ctypes.c_void_p),
+        ("n", ctypes.c_int64),
+        ("invert", ctypes.c_int32),
+        ("has_coset", ctypes.c_int32),
+        ("coset", ctypes.c_uint64 * 4),
+    ]
+
+
 _u64p = ctypes.c_void_p  # device pointers travel as plain addresses
 _i64 = ctypes.c_int64
 _vp = ctypes.c_void_p
 _fp = ctypes.POINTER(ZkbField)
+_jobp = ctypes.POINTER(ZkbMsmJob)
+_nttjobp = ctypes.POINTER(ZkbNttJob)
 
 # name -> (restype, argtypes); the full C ABI of include/zkb200.h
 SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
@@ -68,6 +96,8 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
         [_fp, _u64p, _u64p, _i64, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64),
          ctypes.POINTER(ctypes.c_uint64), _vp, ctypes.c_size_t, _vp],
     ),
+    "zkb_ntt_batch_workspace_bytes": (ctypes.c_size_t, [_nttjobp, ctypes.c_int]),
+    "zkb_ntt_batch": (ctypes.c_int, [_fp, _nttjobp, ctypes.c_int, _vp, ctypes.c_size_t, _vp, _vp]),
     "zkb_g1_add": (ctypes.c_int, [_u64p, _i64, _u64p, _i64, _u64p, _i64, _vp]),
     "zkb_g1_add_affine": (ctypes.c_int, [_u64p, _i64, _u64p, _i64, _u64p, _i64, _vp]),
     "zkb_g1_double": (ctypes.c_int, [_u64p, _u64p, _i64, _vp]),
@@ -79,6 +109,8 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "zkb_msm": (ctypes.c_int, [_u64p, _u64p, _i64, ctypes.c_int, _u64p, _vp, ctypes.c_size_t, _vp]),
     "zkb_msm_no_alloc": (ctypes.c_int, [_u64p, _u64p, _i64, ctypes.c_int, _u64p, _vp]),
     "zkb_msm_no_alloc_capacity": (ctypes.c_size_t, []),
+    "zkb_msm_batch_workspace_bytes": (ctypes.c_size_t, [_jobp, ctypes.c_int]),
+    "zkb_msm_batch": (ctypes.c_int, [_jobp, ctypes.c_int, _vp, ctypes.c_size_t, _vp]),
     "zkb_launch_count": (ctypes.c_uint64, []),
     "zkb_tune_set": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int]),
     "zkb_tune_get": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)]),
