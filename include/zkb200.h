@@ -132,6 +132,15 @@ size_t zkb_ntt_batch_workspace_bytes(const zkb_ntt_job* jobs, int count);
 int zkb_ntt_batch(const zkb_field* f, const zkb_ntt_job* jobs, int count, void* workspace,
                   size_t workspace_bytes, int32_t* status, void* stream);
 
+/* Replaces the quotient step of the reference's GPU prover,
+ * Fr.mul(Fr.sub(Fr.mul(a, b), c), z_inv) (demo/prover_simulation.py:148):
+ * out[i] = (a[i] b[i] - c[i]) z over BN254 Fr, in one pass. a, b, c, out are
+ * (n, 4) Montgomery rows; z points to ONE device row holding z's plain value
+ * (e.g. 1 / (g^n - 1)), so that the call reads nothing from the host. out may
+ * alias a, b or c. */
+int zkb_quotient_pointwise(const uint64_t* a, const uint64_t* b, const uint64_t* c,
+                           const uint64_t* z, uint64_t* out, int64_t n, void* stream);
+
 /* ---- BN254 G1 ------------------------------------------------------------- */
 
 /* Replace the zk_g1_add / zk_g1_add_affine / zk_g1_double launches

@@ -11,6 +11,7 @@ constexpr int kMaxDevices = 64;
 
 struct DeviceSides {
   bool ready = false;
+  int next = 0;  // first side stream of the next fork: calls rotate over them
   cudaStream_t streams[Fanout::kMaxSides] = {};
   cudaEvent_t fork_event = nullptr;
   cudaEvent_t join_events[Fanout::kMaxSides] = {};
@@ -47,20 +48,25 @@ int Fanout::fork(cudaStream_t s, int k) {
   ZKB_TRY(ensure_sides(dev_));
   k_ = k;
   DeviceSides& d = g_sides[dev_];
+  base_ = d.next;
+  d.next = (d.next + k) % kMaxSides;
   ZKB_TRY(check_cuda(cudaEventRecord(d.fork_event, s), "fork record"));
   for (int i = 0; i < k; ++i) {
-    ZKB_TRY(check_cuda(cudaStreamWaitEvent(d.streams[i], d.fork_event, 0), "fork wait"));
+    ZKB_TRY(check_cuda(cudaStreamWaitEvent(side(i), d.fork_event, 0), "fork wait"));
   }
   return ZKB_OK;
 }
 
-cudaStream_t Fanout::side(int i) const { return g_sides[dev_].streams[i % kMaxSides]; }
+cudaStream_t Fanout::side(int i) const {
+  return g_sides[dev_].streams[(base_ + i % k_) % kMaxSides];
+}
 
 int Fanout::join(cudaStream_t s) {
   DeviceSides& d = g_sides[dev_];
   for (int i = 0; i < k_; ++i) {
-    ZKB_TRY(check_cuda(cudaEventRecord(d.join_events[i], d.streams[i]), "join record"));
-    ZKB_TRY(check_cuda(cudaStreamWaitEvent(s, d.join_events[i], 0), "join wait"));
+    const int idx = (base_ + i) % kMaxSides;
+    ZKB_TRY(check_cuda(cudaEventRecord(d.join_events[idx], d.streams[idx]), "join record"));
+    ZKB_TRY(check_cuda(cudaStreamWaitEvent(s, d.join_events[idx], 0), "join wait"));
   }
   k_ = 0;
   return ZKB_OK;
