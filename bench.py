@@ -19,6 +19,14 @@ bound) timed live with CUDA events recorded by the library on its stream;
 `cpu_baseline` is the oracle (a C port of the reference's CPU algorithms)
 timed on a bounded sample on one host core.
 
+Two more objects on the line cover the rest of the metric ("batched jobs/s
+vs plain launches; p99 latency"), on the large workload only:
+`batched` — 64 NTTs + 32 MSMs of uneven sizes as one batch (one persistent
+NTT launch, one MSM batch, and its CUDA-graph replay) against one call per
+job; `served` — a Poisson stream of 2,000 Groth16-shaped prover jobs through
+the continuous-batching server, with p50/p99 latency, against the same jobs
+one at a time.
+
 --impl reference runs the reference's CPU algorithms (the same C port, all
 host threads) on the same workload and prints the same line with
 "impl": "reference".
@@ -381,6 +389,12 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     if not args.skip_e2e:
         e2e = _run_e2e(args, step, dist, device, log_msm, log_ntt)
 
+    batched = served = None
+    if args.workload == "large" and not args.skip_batched:
+        batched = run_batched()
+    if args.workload == "large" and not args.skip_served:
+        served = run_served()
+
     cpu = None
     if rank == 0 and not args.skip_cpu_baseline:
         cpu = cpu_baseline_sample(step, threads=1)
@@ -406,6 +420,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         "clocks": clk,
         "e2e": e2e,
         "cpu_baseline": cpu,
+        "batched": batched,
+        "served": served,
     }
     return line
 
@@ -462,6 +478,135 @@ def _run_e2e(args, step: Step, dist, device, log_msm: int, log_ntt: int) -> dict
     ms = max_over_ranks(a.elapsed_time(b) / steps, dist, device)
     return {"value": round(ms, 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
             "steps": steps, "api": "zkgpu.msm_gpu.msm_pippenger_affine x2, Field256.to_montgomery/ntt/from_montgomery x2"}
+
+
+# ------------------------------------------------------------------
+# Batched form (64 NTTs + 32 MSMs) and served form (Poisson stream of prover jobs)
+# ------------------------------------------------------------------
+
+
+def _event_ms(fn, reps: int) -> float:
+    import torch
+
+    for _ in range(2):
+        fn()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        fn()
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+def run_batched(seed: int = 6, log_base: int = 20) -> dict:
+    """64 Fr NTTs (sizes 2^U{10..20}, uniform inputs) + 32 G1 MSMs (sizes 2^U(12, 20) over
+    prefixes of one resident 2^20 base set, uniform scalars): one-at-a-time calls against one
+    BatchPlan run (one persistent NTT launch + one MSM batch) and its CUDA-graph replay."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    from zkgpu import _native, batch, curve_gpu, workloads as wl
+    from zkgpu.field256_gpu import BN254_FR
+
+    rng = np.random.default_rng(seed)
+    ntt_sizes = [1 << int(v) for v in rng.integers(10, log_base + 1, size=64)]
+    msm_sizes = [int(2 ** v) for v in rng.uniform(12, log_base, size=32)]
+    bases = curve_gpu.mul_generator(wl.base_scalars(seed, 1 << log_base))
+    xs = [BN254_FR.to_montgomery(wl.uniform_fr(1000 + k, n)) for k, n in enumerate(ntt_sizes)]
+    scs = [torch.from_numpy(wl.uniform_fr(2000 + k, n)).cuda() for k, n in enumerate(msm_sizes)]
+    lib = _native.lib()
+    f = BN254_FR._field()
+    outs = [torch.empty_like(x) for x in xs]
+    ntt_ws = [_native.workspace(lib.zkb_ntt_workspace_bytes(n)) for n in ntt_sizes]
+    msm_ws = [_native.workspace(lib.zkb_msm_workspace_bytes(n, 0)) for n in msm_sizes]
+    res = torch.empty((32, 16), dtype=torch.int64, device="cuda")
+
+    def plain() -> None:
+        s = _native.stream_ptr()
+        for k, n in enumerate(ntt_sizes):
+            _native.check(lib.zkb_ntt(ctypes.byref(f), xs[k].data_ptr(), outs[k].data_ptr(), n, 0, None, None,
+                                      ntt_ws[k].data_ptr(), ntt_ws[k].numel(), s))
+        for k, n in enumerate(msm_sizes):
+            _native.check(lib.zkb_msm(bases.data_ptr(), scs[k].data_ptr(), n, 0, res[k].data_ptr(),
+                                      msm_ws[k].data_ptr(), msm_ws[k].numel(), s))
+
+    plan = batch.BatchPlan(ntt_jobs=[(x, False, None) for x in xs],
+                           msm_jobs=[(bases[:n], scs[k], None) for k, n in enumerate(msm_sizes)])
+    t_plain = _event_ms(plain, 3)
+    t_batch = _event_ms(plan.run, 3)
+    same = all(bool((o == y).all()) for o, y in zip(outs, plan.ntt_outputs)) and \
+        bool((res[:, :9] == plan.msm_results[:32, :9]).all())
+    plan.capture()
+    t_graph = _event_ms(plan.replay, 3)
+    plan.check_status()
+    same = same and all(bool((o == y).all()) for o, y in zip(outs, plan.ntt_outputs)) and \
+        bool((res[:, :9] == plan.msm_results[:32, :9]).all())
+    jobs = len(ntt_sizes) + len(msm_sizes)
+    return {
+        "workload": f"64 Fr NTTs 2^U{{10..{log_base}}} + 32 G1 MSMs 2^U(12,{log_base}) over one resident "
+                    f"2^{log_base} base set (seed {seed})",
+        "jobs": jobs, "plain_ms": round(t_plain, 3), "batched_ms": round(t_batch, 3), "graph_ms": round(t_graph, 3),
+        "plain_jobs_per_s": round(jobs / t_plain * 1e3, 1), "batched_jobs_per_s": round(jobs / t_batch * 1e3, 1),
+        "graph_jobs_per_s": round(jobs / t_graph * 1e3, 1), "speedup": round(t_plain / min(t_batch, t_graph), 3),
+        "launches_per_batch": plan.launches_per_run, "same_results": same,
+        "timing": "CUDA events, mean of 3 after 2 warm-up",
+    }
+
+
+def run_served(n_jobs: int = 2000, rate: float = 200.0, log_max: int = 20, seed: int = 7) -> dict:
+    """Poisson stream (rate jobs/s) of Groth16-shaped jobs, m = 2^U{12..log_max}: each job 3
+    inverse NTTs, 3 coset NTTs, the pointwise quotient, 1 inverse coset NTT and 4 G1 MSMs
+    (skewed witness scalars; h for the last) over a resident base set. The served form
+    (zkgpu.serving) against the same jobs one at a time (prove_plain, a 60-job sample)."""
+    import numpy as np
+    import torch
+
+    from zkgpu import curve_gpu, workloads as wl
+    from zkgpu.prover import ProofJob, prove_plain, synthetic_request
+    from zkgpu.serving import Server, summarize
+
+    bases = curve_gpu.mul_generator(wl.base_scalars(seed, 1 << log_max))
+    pool = {1 << e: [synthetic_request(1000 * e + k, 1 << e) for k in range(2)] for e in range(12, log_max + 1)}
+    rng = np.random.default_rng(seed)
+    exps = rng.integers(12, log_max + 1, size=n_jobs)
+    reqs = [pool[1 << int(e)][k % 2] for k, e in enumerate(exps)]
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n_jobs))
+    for group in pool.values():
+        for q in group:
+            q.host_rows()
+    sample = reqs[: min(60, n_jobs)]
+    ws: dict = {}
+    for r in sample[:3]:
+        prove_plain(ProofJob(r, bases), ws)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for r in sample:
+        prove_plain(ProofJob(r, bases), ws)
+        torch.cuda.synchronize()
+    plain_s = time.perf_counter() - t0
+    budget = 60 << 30
+    Server(bases, budget).run(sample[:10], [0.0] * 10)  # warm-up: tables, allocator
+    srv = Server(bases, budget)
+    t0 = time.perf_counter()
+    recs = srv.run(reqs, list(arrivals))
+    wall = time.perf_counter() - t0
+    s = summarize(recs, wall)
+    plain_jobs_s = len(sample) / plain_s
+    return {
+        "workload": f"{n_jobs} Groth16-shaped jobs, Poisson {rate:g}/s, m = 2^U{{12..{log_max}}}, 7 NTTs + "
+                    f"4 G1 MSMs each, resident 2^{log_max} base set (seed {seed})",
+        "jobs": n_jobs, "rate_per_s": rate, "jobs_per_s": round(s["jobs_per_s"], 1),
+        "p50_ms": round(s["p50_ms"], 2), "p90_ms": round(s["p90_ms"], 2), "p99_ms": round(s["p99_ms"], 2),
+        "max_ms": round(s["max_ms"], 2), "plain_jobs_per_s": round(plain_jobs_s, 1),
+        "speedup_vs_plain": round(s["jobs_per_s"] / plain_jobs_s, 3),
+        "plain": f"the first {len(sample)} jobs one at a time (one call per NTT / MSM, synchronised per job)",
+        "ticks": srv.ticks, "gpu_launches": srv.launches, "hbm_budget_bytes": budget,
+        "latency": "arrival (host clock) to the device-side completion of the job's last MSM batch",
+    }
 
 
 # ------------------------------------------------------------------
@@ -591,6 +736,8 @@ def main() -> None:
     ap.add_argument("--workload", choices=tuple(WORKLOADS), default="large")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu-baseline", action="store_true")
+    ap.add_argument("--skip-batched", action="store_true", help="skip the batched form (64 NTTs + 32 MSMs)")
+    ap.add_argument("--skip-served", action="store_true", help="skip the served form (Poisson job stream)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3  # at least three untimed steps
