@@ -122,6 +122,23 @@ def test_heavy_bucket_and_boolean_scalars():
     assert msm_pippenger_gpu(xs, ys, [int(b) for b in bools], window_size=9) == Point(*want)
 
 
+@pytest.mark.parametrize("case", golden("msm.json")["seeded"][:2], ids=lambda c: f"{c['kind']}-{c['n']}")
+def test_inlined_products_give_the_same_point(case):
+    """The bucket, merge, reduction and finalize kernels compiled with every product expanded
+    in place (msm.call_products = 0) give the reference's point as the default shared-product
+    kernels do."""
+    n = case["n"]
+    bases = _bases(n, case["base_seed"])
+    gen = wl.uniform_fr if case["kind"] == "uniform" else wl.skewed_scalars
+    sc = gen(case["scalar_seed"], n)
+    try:
+        _native.tune_set("msm.call_products", 0)
+        for w in (None, 7):
+            assert msm_pippenger_rows(bases, sc, window_size=w) == expected_point(case), w
+    finally:
+        _native.tune_set("msm.call_products", 1)
+
+
 def test_self_test_passes():
     msm_gpu.compile_kernels()
 

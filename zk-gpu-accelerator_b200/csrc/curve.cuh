@@ -237,24 +237,44 @@ __device__ __forceinline__ void xyzz_from_affine(Xyzz& r, const Aff& q) {
   fe_one(r.zzz, f);
 }
 
+// Products in the XYZZ formulas go through a policy M: InlineMul expands
+// every Montgomery product in place; CallMul calls one shared copy of it.
+// The bucket kernels run one mixed addition per sorted pair in a loop; with
+// its ten products (and the rare doubling path's eight) expanded, the loop
+// body outgrows the SM's instruction cache and warps stall on instruction
+// fetch. With CallMul the body calls one shared copy of the product
+// (fe_mul_shared).
+struct InlineMul {
+  __device__ __forceinline__ static void mul(uint32_t r[8], const uint32_t a[8], const uint32_t b[8]) {
+    fe_mul(r, a, b, G1F{});
+  }
+};
+
+struct CallMul {
+  __device__ __forceinline__ static void mul(uint32_t r[8], const uint32_t a[8], const uint32_t b[8]) {
+    fe_mul_shared(r, a, b, G1F{});
+  }
+};
+
 // 2(x, y) for an affine point, mdbl-2008-s-1: U = 2y, V = U^2, W = U V,
 // S = x V, M = 3 x^2, X3 = M^2 - 2S, Y3 = M (S - X3) - W y, ZZ3 = V, ZZZ3 = W.
+template <class M = InlineMul>
 __device__ __forceinline__ void xyzz_mdbl(Xyzz& r, const Aff& q) {
   G1F f;
   uint32_t u[8], v[8], w[8], s[8], m[8], t[8];
   fe_dbl(u, q.y, f);
-  fe_sqr(v, u, f);
-  fe_mul(w, u, v, f);
-  fe_mul(s, q.x, v, f);
-  fe_sqr(m, q.x, f);
+  M::mul(v, u, u);
+  M::mul(w, u, v);
+  M::mul(s, q.x, v);
+  M::mul(m, q.x, q.x);
   fe_dbl(t, m, f);
   fe_add(m, m, t, f);
-  fe_sqr(r.x, m, f);
+  M::mul(r.x, m, m);
   fe_dbl(t, s, f);
   fe_sub(r.x, r.x, t, f);
   fe_sub(t, s, r.x, f);
-  fe_mul(r.y, m, t, f);
-  fe_mul(t, w, q.y, f);
+  M::mul(r.y, m, t);
+  M::mul(t, w, q.y);
   fe_sub(r.y, r.y, t, f);
   fe_copy(r.zz, v);
   fe_copy(r.zzz, w);
@@ -262,6 +282,7 @@ __device__ __forceinline__ void xyzz_mdbl(Xyzz& r, const Aff& q) {
 
 // 2P, dbl-2008-s-1 (a = 0): U = 2Y, V = U^2, W = U V, S = X V, M = 3 X^2,
 // X3 = M^2 - 2S, Y3 = M (S - X3) - W Y, ZZ3 = V ZZ, ZZZ3 = W ZZZ.
+template <class M = InlineMul>
 __device__ __forceinline__ void xyzz_dbl(Xyzz& r, const Xyzz& p) {
   G1F f;
   if (fe_is_zero(p.zz) || fe_is_zero(p.y)) {
@@ -270,22 +291,22 @@ __device__ __forceinline__ void xyzz_dbl(Xyzz& r, const Xyzz& p) {
   }
   uint32_t u[8], v[8], w[8], s[8], m[8], t[8];
   fe_dbl(u, p.y, f);
-  fe_sqr(v, u, f);
-  fe_mul(w, u, v, f);
-  fe_mul(s, p.x, v, f);
-  fe_sqr(m, p.x, f);
+  M::mul(v, u, u);
+  M::mul(w, u, v);
+  M::mul(s, p.x, v);
+  M::mul(m, p.x, p.x);
   fe_dbl(t, m, f);
   fe_add(m, m, t, f);
   uint32_t x3[8], y3[8];
-  fe_sqr(x3, m, f);
+  M::mul(x3, m, m);
   fe_dbl(t, s, f);
   fe_sub(x3, x3, t, f);
   fe_sub(t, s, x3, f);
-  fe_mul(y3, m, t, f);
-  fe_mul(t, w, p.y, f);
+  M::mul(y3, m, t);
+  M::mul(t, w, p.y);
   fe_sub(y3, y3, t, f);
-  fe_mul(r.zz, v, p.zz, f);
-  fe_mul(r.zzz, w, p.zzz, f);
+  M::mul(r.zz, v, p.zz);
+  M::mul(r.zzz, w, p.zzz);
   fe_copy(r.x, x3);
   fe_copy(r.y, y3);
 }
@@ -294,6 +315,7 @@ __device__ __forceinline__ void xyzz_dbl(Xyzz& r, const Xyzz& p) {
 // PPP = P' PP, Q = X1 PP, X3 = R^2 - PPP - 2Q, Y3 = R (Q - X3) - Y1 PPP,
 // ZZ3 = ZZ1 PP, ZZZ3 = ZZZ1 PPP. Special cases: P the identity gives Q;
 // P' = 0 means equal x: doubling (R = 0) or the identity (R != 0).
+template <class M = InlineMul>
 __device__ __forceinline__ void xyzz_add_affine(Xyzz& acc, const Aff& q) {
   G1F f;
   if (fe_is_zero(acc.zz)) {
@@ -301,31 +323,31 @@ __device__ __forceinline__ void xyzz_add_affine(Xyzz& acc, const Aff& q) {
     return;
   }
   uint32_t pp[8], r[8], t[8];
-  fe_mul(pp, q.x, acc.zz, f);
+  M::mul(pp, q.x, acc.zz);
   fe_sub(pp, pp, acc.x, f);   // P'
-  fe_mul(r, q.y, acc.zzz, f);
+  M::mul(r, q.y, acc.zzz);
   fe_sub(r, r, acc.y, f);     // R
   if (fe_is_zero(pp)) {
     if (fe_is_zero(r)) {
-      xyzz_mdbl(acc, q);
+      xyzz_mdbl<M>(acc, q);
     } else {
       xyzz_set_identity(acc);
     }
     return;
   }
   uint32_t ppp[8], qq[8];
-  fe_sqr(t, pp, f);           // PP
-  fe_mul(ppp, pp, t, f);      // PPP
-  fe_mul(qq, acc.x, t, f);    // Q
-  fe_mul(acc.zz, acc.zz, t, f);
-  fe_mul(acc.zzz, acc.zzz, ppp, f);
-  fe_sqr(t, r, f);
+  M::mul(t, pp, pp);           // PP
+  M::mul(ppp, pp, t);      // PPP
+  M::mul(qq, acc.x, t);    // Q
+  M::mul(acc.zz, acc.zz, t);
+  M::mul(acc.zzz, acc.zzz, ppp);
+  M::mul(t, r, r);
   fe_sub(t, t, ppp, f);
   fe_sub(t, t, qq, f);
   fe_sub(t, t, qq, f);        // X3
   fe_sub(qq, qq, t, f);
-  fe_mul(qq, r, qq, f);       // R (Q - X3)
-  fe_mul(ppp, acc.y, ppp, f); // Y1 PPP
+  M::mul(qq, r, qq);       // R (Q - X3)
+  M::mul(ppp, acc.y, ppp); // Y1 PPP
   fe_sub(acc.y, qq, ppp, f);
   fe_copy(acc.x, t);
 }
@@ -334,6 +356,7 @@ __device__ __forceinline__ void xyzz_add_affine(Xyzz& acc, const Aff& q) {
 // P' = U2 - U1, R = S2 - S1, PP = P'^2, PPP = P' PP, Q = U1 PP,
 // X3 = R^2 - PPP - 2Q, Y3 = R (Q - X3) - S1 PPP, ZZ3 = ZZ1 ZZ2 PP,
 // ZZZ3 = ZZZ1 ZZZ2 PPP. r may alias p or q.
+template <class M = InlineMul>
 __device__ __forceinline__ void xyzz_add(Xyzz& r, const Xyzz& p, const Xyzz& q) {
   G1F f;
   if (fe_is_zero(q.zz)) {
@@ -345,35 +368,35 @@ __device__ __forceinline__ void xyzz_add(Xyzz& r, const Xyzz& p, const Xyzz& q) 
     return;
   }
   uint32_t u1[8], s1[8], pp[8], rr[8], t[8];
-  fe_mul(u1, p.x, q.zz, f);
-  fe_mul(pp, q.x, p.zz, f);
+  M::mul(u1, p.x, q.zz);
+  M::mul(pp, q.x, p.zz);
   fe_sub(pp, pp, u1, f);      // P'
-  fe_mul(s1, p.y, q.zzz, f);
-  fe_mul(rr, q.y, p.zzz, f);
+  M::mul(s1, p.y, q.zzz);
+  M::mul(rr, q.y, p.zzz);
   fe_sub(rr, rr, s1, f);      // R
   if (fe_is_zero(pp)) {
     if (fe_is_zero(rr)) {
-      xyzz_dbl(r, p);
+      xyzz_dbl<M>(r, p);
     } else {
       xyzz_set_identity(r);
     }
     return;
   }
   uint32_t ppp[8], qq[8], zz[8], zzz[8];
-  fe_sqr(t, pp, f);           // PP
-  fe_mul(ppp, pp, t, f);      // PPP
-  fe_mul(qq, u1, t, f);       // Q
-  fe_mul(zz, p.zz, q.zz, f);
-  fe_mul(zz, zz, t, f);
-  fe_mul(zzz, p.zzz, q.zzz, f);
-  fe_mul(zzz, zzz, ppp, f);
-  fe_sqr(t, rr, f);
+  M::mul(t, pp, pp);           // PP
+  M::mul(ppp, pp, t);      // PPP
+  M::mul(qq, u1, t);       // Q
+  M::mul(zz, p.zz, q.zz);
+  M::mul(zz, zz, t);
+  M::mul(zzz, p.zzz, q.zzz);
+  M::mul(zzz, zzz, ppp);
+  M::mul(t, rr, rr);
   fe_sub(t, t, ppp, f);
   fe_sub(t, t, qq, f);
   fe_sub(t, t, qq, f);        // X3
   fe_sub(qq, qq, t, f);
-  fe_mul(qq, rr, qq, f);
-  fe_mul(s1, s1, ppp, f);
+  M::mul(qq, rr, qq);
+  M::mul(s1, s1, ppp);
   fe_sub(r.y, qq, s1, f);
   fe_copy(r.x, t);
   fe_copy(r.zz, zz);

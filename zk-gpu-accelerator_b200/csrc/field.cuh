@@ -365,6 +365,44 @@ __device__ __forceinline__ void fe_sqr(uint32_t r[8], const uint32_t a[8], const
   fe_mul(r, a, a, f);
 }
 
+// ---- one shared copy of the product ----------------------------------------
+// Kernels whose loop bodies hold many products (the bucket additions, the NTT
+// butterflies) outgrow the SM's instruction cache when every product is
+// expanded in place, and their warps then stall on instruction fetch.
+// fe_mul_shared calls one out-of-line copy of the product per field instead;
+// the operands travel by value in registers (no stack frame), so a call adds
+// a few register moves to the ~470 instructions of the product. Fields with
+// a modulus known only at run time keep the inline product.
+struct Fe8 {
+  uint32_t w[8];
+};
+
+template <class F>
+static __device__ __noinline__ Fe8 fe_mul_outlined(const Fe8 a, const Fe8 b) {
+  Fe8 r;
+  fe_mul(r.w, a.w, b.w, F{});
+  return r;
+}
+
+template <class F>
+__device__ __forceinline__ void fe_mul_shared(uint32_t r[8], const uint32_t a[8],
+                                              const uint32_t b[8], const F&) {
+  Fe8 x, y;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    x.w[j] = a[j];
+    y.w[j] = b[j];
+  }
+  const Fe8 z = fe_mul_outlined<F>(x, y);
+#pragma unroll
+  for (int j = 0; j < 8; ++j) r[j] = z.w[j];
+}
+
+__device__ __forceinline__ void fe_mul_shared(uint32_t r[8], const uint32_t a[8],
+                                              const uint32_t b[8], const FieldRT& f) {
+  fe_mul(r, a, b, f);
+}
+
 // r = 2a, 3a, 4a, 8a mod p.
 template <class F>
 __device__ __forceinline__ void fe_dbl(uint32_t r[8], const uint32_t a[8], const F& f) {

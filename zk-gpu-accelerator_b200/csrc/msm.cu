@@ -387,7 +387,7 @@ __device__ __forceinline__ JobPoints job_points(const MsmJobs& J, uint32_t key) 
 // Level 1: K1 sorted (key, value) pairs per thread, mixed additions of affine
 // input points. kBatch = false is the one-job form: the job lookup at each
 // new run costs 40+ registers, so a single MSM keeps its point arrays fixed.
-template <bool kBatch>
+template <bool kBatch, class M>
 __device__ __forceinline__ void acc_points(const MsmJobs& J, const uint32_t* keys,
                                            const uint32_t* vals, int64_t E, int K, uint32_t none,
                                            uint64_t* buckets, uint32_t* slot_keys,
@@ -421,21 +421,23 @@ __device__ __forceinline__ void acc_points(const MsmJobs& J, const uint32_t* key
     Aff q;
     aff_load_nc(q, idx < jp.n ? jp.points + 8 * idx : jp.phi + 8 * (idx - jp.n));
     if (v >> 31) aff_neg(q);
-    xyzz_add_affine(acc, q);
+    xyzz_add_affine<M>(acc, q);
   }
   if (cur != none) sink.flush(cur, acc, first, true);
 }
 
 // One MSM (108 registers, four CTAs per SM).
+template <class M>
 __global__ void __launch_bounds__(128) k_msm_acc_points(const MsmJobs J, const uint32_t* keys,
                                                         const uint32_t* vals, int64_t E, int K,
                                                         uint32_t none, uint64_t* buckets,
                                                         uint32_t* slot_keys, uint64_t* slot_pts) {
-  acc_points<false>(J, keys, vals, E, K, none, buckets, slot_keys, slot_pts);
+  acc_points<false, M>(J, keys, vals, E, K, none, buckets, slot_keys, slot_pts);
 }
 
 // A batch: capped at 128 registers (a few bytes of spill on the job-change
 // path) to keep four CTAs per SM.
+template <class M>
 __global__ void __launch_bounds__(128, 4) k_msm_acc_points_batch(const MsmJobs J,
                                                                  const uint32_t* keys,
                                                                  const uint32_t* vals, int64_t E,
@@ -443,11 +445,12 @@ __global__ void __launch_bounds__(128, 4) k_msm_acc_points_batch(const MsmJobs J
                                                                  uint64_t* buckets,
                                                                  uint32_t* slot_keys,
                                                                  uint64_t* slot_pts) {
-  acc_points<true>(J, keys, vals, E, K, none, buckets, slot_keys, slot_pts);
+  acc_points<true, M>(J, keys, vals, E, K, none, buckets, slot_keys, slot_pts);
 }
 
 // Levels 2+: K2 slots per thread, full XYZZ additions; slots without a key
 // (none) may sit anywhere between runs and are skipped.
+template <class Mul>
 __global__ void __launch_bounds__(128) k_msm_acc_slots(const uint32_t* in_keys,
                                                        const uint64_t* in_pts, int64_t M, int K,
                                                        uint32_t none, uint64_t* buckets,
@@ -476,7 +479,7 @@ __global__ void __launch_bounds__(128) k_msm_acc_slots(const uint32_t* in_keys,
     if (k == none) continue;
     Xyzz q;
     xyzz_load(q, in_pts + 16 * e);
-    xyzz_add(acc, acc, q);
+    xyzz_add<Mul>(acc, acc, q);
   }
   sink.flush(cur, acc, first, true);
 }
@@ -487,6 +490,7 @@ __global__ void __launch_bounds__(128) k_msm_acc_slots(const uint32_t* in_keys,
 
 // One thread per (window, segment). X and U_in are [W][G_in]; outputs are
 // [W][G_in / L] (S scaled by L), or the window sums at the last level.
+template <class Mul>
 __global__ void __launch_bounds__(128) k_msm_reduce(const uint64_t* X, const uint64_t* U_in,
                                                     int64_t G_in, int lL, int delta, int W,
                                                     uint64_t* S_out, uint64_t* U_out,
@@ -503,18 +507,18 @@ __global__ void __launch_bounds__(128) k_msm_reduce(const uint64_t* X, const uin
   xyzz_set_identity(tot);
   for (int64_t i = len - 1; i >= 0; --i) {
     xyzz_load(x, X + 16 * (base + i));
-    xyzz_add(running, running, x);
-    if (i > 0 || delta) xyzz_add(tot, tot, running);
+    xyzz_add<Mul>(running, running, x);
+    if (i > 0 || delta) xyzz_add<Mul>(tot, tot, running);
   }
   if (U_in) {
     for (int64_t i = 0; i < len; ++i) {
       xyzz_load(x, U_in + 16 * (base + i));
-      xyzz_add(tot, tot, x);
+      xyzz_add<Mul>(tot, tot, x);
     }
   }
   xyzz_store(U_out + 16 * (win * G_out + t), tot);
   if (!final_level) {
-    for (int k = 0; k < lL; ++k) xyzz_dbl(running, running);
+    for (int k = 0; k < lL; ++k) xyzz_dbl<Mul>(running, running);
     xyzz_store(S_out + 16 * (win * G_out + t), running);
   }
 }
@@ -526,6 +530,7 @@ __global__ void __launch_bounds__(128) k_msm_reduce(const uint64_t* X, const uin
 // One thread per job. Horner from the top window: acc = 2^w acc + S_win; then
 // affine x = X / ZZ, y = Y / ZZZ with one inversion of ZZ ZZZ, as plain
 // canonical values.
+template <class Mul>
 __global__ void k_msm_finalize(const MsmJobs J, const uint64_t* all_window_sums, int W, int w) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= J.count) return;
@@ -535,9 +540,9 @@ __global__ void k_msm_finalize(const MsmJobs J, const uint64_t* all_window_sums,
   Xyzz acc, s;
   xyzz_load(acc, window_sums + 16 * (W - 1));
   for (int win = W - 2; win >= 0; --win) {
-    for (int k = 0; k < w; ++k) xyzz_dbl(acc, acc);
+    for (int k = 0; k < w; ++k) xyzz_dbl<Mul>(acc, acc);
     xyzz_load(s, window_sums + 16 * win);
-    xyzz_add(acc, acc, s);
+    xyzz_add<Mul>(acc, acc, s);
   }
   uint32_t x[8], y[8];
   uint64_t flag = 0;
@@ -605,6 +610,7 @@ struct MsmPlan {
   int k1 = 64;     // sorted pairs per bucket thread ("msm.pairs_per_thread")
   int k2 = 8;      // slots per merge thread ("msm.slots_per_thread")
   int log_l = 2;   // log2 running-sum segment ("msm.reduce_log_segment")
+  int call_products = 1;  // bucket kernels call one shared product ("msm.call_products")
   int64_t E = 0;   // sorted pairs
   int64_t T1 = 0;  // level-1 threads
   std::vector<int64_t> slot_levels;  // thread count of each merge level
@@ -634,6 +640,7 @@ static int make_plan(const int64_t* sizes, int count, int w, MsmPlan& p) {
   p.k1 = tune_get("msm.pairs_per_thread");
   p.k2 = tune_get("msm.slots_per_thread");
   p.log_l = tune_get("msm.reduce_log_segment");
+  p.call_products = tune_get("msm.call_products");
   p.T1 = (p.E + p.k1 - 1) / p.k1;
   p.slot_levels.clear();
   int64_t M = 2 * p.T1;
@@ -739,11 +746,11 @@ static int run_msm(const MsmJobs& J, const MsmPlan& p, char* ws, cudaStream_t s)
     ProfSpan span("msm_acc_points", s);
     const unsigned grid = (unsigned)((p.T1 + 127) / 128);
     if (p.count > 1) {
-      k_msm_acc_points_batch<<<grid, 128, 0, s>>>(J, skeys, svals, p.E, p.k1, p.none, buckets,
-                                                  sk[0], sp[0]);
+      auto kern = p.call_products ? k_msm_acc_points_batch<CallMul> : k_msm_acc_points_batch<InlineMul>;
+      kern<<<grid, 128, 0, s>>>(J, skeys, svals, p.E, p.k1, p.none, buckets, sk[0], sp[0]);
     } else {
-      k_msm_acc_points<<<grid, 128, 0, s>>>(J, skeys, svals, p.E, p.k1, p.none, buckets, sk[0],
-                                            sp[0]);
+      auto kern = p.call_products ? k_msm_acc_points<CallMul> : k_msm_acc_points<InlineMul>;
+      kern<<<grid, 128, 0, s>>>(J, skeys, svals, p.E, p.k1, p.none, buckets, sk[0], sp[0]);
     }
     ZKB_TRY(check_launch("msm bucket accumulation"));
   }
@@ -754,7 +761,8 @@ static int run_msm(const MsmJobs& J, const MsmPlan& p, char* ws, cudaStream_t s)
     for (size_t lvl = 0; lvl < p.slot_levels.size(); ++lvl) {
       const int64_t T = p.slot_levels[lvl];
       const unsigned grid = (unsigned)((T + 127) / 128);
-      k_msm_acc_slots<<<grid, 128, 0, s>>>(sk[cur], sp[cur], M, p.k2, p.none, buckets,
+      auto kern = p.call_products ? k_msm_acc_slots<CallMul> : k_msm_acc_slots<InlineMul>;
+      kern<<<grid, 128, 0, s>>>(sk[cur], sp[cur], M, p.k2, p.none, buckets,
                                            sk[cur ^ 1], sp[cur ^ 1]);
       ZKB_TRY(check_launch("msm bucket merge"));
       cur ^= 1;
@@ -778,7 +786,8 @@ static int run_msm(const MsmJobs& J, const MsmPlan& p, char* ws, cudaStream_t s)
     while (G > L) {
       const int64_t G_out = G / L;
       const int64_t threads = windows * G_out;
-      k_msm_reduce<<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(X, U, G, p.log_l, delta,
+      auto red = p.call_products ? k_msm_reduce<CallMul> : k_msm_reduce<InlineMul>;
+      red<<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(X, U, G, p.log_l, delta,
                                                                      (int)windows, rs[r], ru[r], 0);
       ZKB_TRY(check_launch("msm window reduction"));
       X = rs[r];
@@ -787,14 +796,16 @@ static int run_msm(const MsmJobs& J, const MsmPlan& p, char* ws, cudaStream_t s)
       G = G_out;
       delta = 0;
     }
-    k_msm_reduce<<<(unsigned)((windows + 127) / 128), 128, 0, s>>>(X, U, G, p.log_l, delta,
+    auto red = p.call_products ? k_msm_reduce<CallMul> : k_msm_reduce<InlineMul>;
+    red<<<(unsigned)((windows + 127) / 128), 128, 0, s>>>(X, U, G, p.log_l, delta,
                                                                    (int)windows, nullptr, wsum, 1);
     ZKB_TRY(check_launch("msm window sums"));
   }
 
   // 5. finalize
   ProfSpan fin_span("msm_finalize", s);
-  k_msm_finalize<<<1, p.count < 32 ? 32 : p.count, 0, s>>>(J, wsum, p.W, p.w);
+  auto fin = p.call_products ? k_msm_finalize<CallMul> : k_msm_finalize<InlineMul>;
+  fin<<<1, p.count < 32 ? 32 : p.count, 0, s>>>(J, wsum, p.W, p.w);
   return check_launch("msm finalize");
 }
 

@@ -274,20 +274,33 @@ __device__ __forceinline__ int sm_index(int c, int j, int lr) {
   return c * ((4 << lr) + 2) + 4 * (j ^ ((j >> 2) & 3));
 }
 
-template <class F>
+// Products of the pass kernel: one shared out-of-line copy (kShared, the
+// default: the expanded products of a radix-4 round and the store path
+// overflow the instruction cache) or expanded in place.
+template <bool kShared, class F>
+__device__ __forceinline__ void ntt_mul(uint32_t r[8], const uint32_t a[8], const uint32_t b[8],
+                                        const F& f) {
+  if (kShared) {
+    fe_mul_shared(r, a, b, f);
+  } else {
+    fe_mul(r, a, b, f);
+  }
+}
+
+template <bool kShared, class F>
 __device__ __forceinline__ void root_power(uint32_t r[8], const NttPass& a, uint64_t e, const F& f) {
   // w_N^e for 0 <= e < N
   const uint64_t mask = (1ull << a.s) - 1;
   uint32_t lo[8], hi[8];
   fe_load_nc(lo, a.t_lo + 4 * (e & mask));
   fe_load_nc(hi, a.t_hi + 4 * (e >> a.s));
-  fe_mul(r, lo, hi, f);
+  ntt_mul<kShared>(r, lo, hi, f);
 }
 
 // One tile (CTA-sized piece) `bid` of pass a. kFresh: the pass reads rows
 // that other CTAs wrote earlier in the same kernel (the batched form), so its
 // row loads bypass L1.
-template <class F, bool kFresh>
+template <class F, bool kFresh, bool kShared>
 __device__ __forceinline__ void ntt_tile(const F& f, const NttPass& a, int64_t bid,
                                          uint64_t* sm) {
   const int lr = a.lr, lc = a.lc;
@@ -346,8 +359,8 @@ __device__ __forceinline__ void ntt_tile(const F& f, const NttPass& a, int64_t b
       uint32_t lo[8], hi[8];
       fe_load_nc(lo, a.g_lo + 4 * ((uint64_t)pos & m));
       fe_load_nc(hi, a.g_hi + 4 * ((uint64_t)pos >> a.gs));
-      fe_mul(lo, lo, hi, f);
-      fe_mul(x, x, lo, f);
+      ntt_mul<kShared>(lo, lo, hi, f);
+      ntt_mul<kShared>(x, x, lo, f);
     }
     fe_store(sm + sm_index(c, jr, lr), x);
   }
@@ -374,8 +387,8 @@ __device__ __forceinline__ void ntt_tile(const F& f, const NttPass& a, int64_t b
       fe_load(x3, sm + sm_index(c, i0 + 3 * h, lr));
       if (st > 0) {
         fe_load(w, tw + 4 * (jj << (lr - 1 - st)));  // w_2h^jj
-        fe_mul(x1, x1, w, f);
-        fe_mul(x3, x3, w, f);
+        ntt_mul<kShared>(x1, x1, w, f);
+        ntt_mul<kShared>(x3, x3, w, f);
       }
       fe_add(t, x0, x1, f);
       fe_sub(x1, x0, x1, f);
@@ -385,10 +398,10 @@ __device__ __forceinline__ void ntt_tile(const F& f, const NttPass& a, int64_t b
       fe_copy(x2, t);
       if (st > 0) {
         fe_load(w, tw + 4 * (jj << (lr - 2 - st)));  // w_4h^jj
-        fe_mul(x2, x2, w, f);
+        ntt_mul<kShared>(x2, x2, w, f);
       }
       fe_load(w, tw + 4 * ((jj + h) << (lr - 2 - st)));  // w_4h^(jj + h)
-      fe_mul(x3, x3, w, f);
+      ntt_mul<kShared>(x3, x3, w, f);
       fe_add(t, x0, x2, f);
       fe_sub(x2, x0, x2, f);
       fe_store(sm + sm_index(c, i0, lr), t);
@@ -413,7 +426,7 @@ __device__ __forceinline__ void ntt_tile(const F& f, const NttPass& a, int64_t b
       fe_load(v, sm + sm_index(c, i0 + h, lr));
       if (st > 0) {
         fe_load(w, tw + 4 * (jj << (lr - 1 - st)));
-        fe_mul(v, v, w, f);
+        ntt_mul<kShared>(v, v, w, f);
       }
       fe_add(x, u, v, f);
       fe_sub(v, u, v, f);
@@ -436,8 +449,8 @@ __device__ __forceinline__ void ntt_tile(const F& f, const NttPass& a, int64_t b
       if (a.inverse && e) e = (1ull << a.log_N) - e;
       if (e) {
         uint32_t tw[8];
-        root_power(tw, a, e, f);
-        fe_mul(x, x, tw, f);
+        root_power<kShared>(tw, a, e, f);
+        ntt_mul<kShared>(x, x, tw, f);
       }
       const int64_t pos = o * B + (int64_t)k * S + jp;
       fe_store(a.out + 4 * pos, x);
@@ -452,21 +465,21 @@ __device__ __forceinline__ void ntt_tile(const F& f, const NttPass& a, int64_t b
           uint32_t lo[8], hi[8];
           fe_load_nc(lo, a.g_lo + 4 * ((uint64_t)outidx & m));
           fe_load_nc(hi, a.g_hi + 4 * ((uint64_t)outidx >> a.gs));
-          fe_mul(sc, lo, hi, f);
+          ntt_mul<kShared>(sc, lo, hi, f);
         } else {
           fe_load_nc(sc, a.scale);
         }
-        fe_mul(x, x, sc, f);
+        ntt_mul<kShared>(x, x, sc, f);
       }
       fe_store(a.out + 4 * outidx, x);
     }
   }
 }
 
-template <class F>
+template <class F, bool kShared>
 __global__ void __launch_bounds__(kNttThreads, 1) k_ntt_pass(F f, NttPass a) {
   extern __shared__ uint4 smem_raw[];
-  ntt_tile<F, false>(f, a, blockIdx.x, reinterpret_cast<uint64_t*>(smem_raw));
+  ntt_tile<F, false, kShared>(f, a, blockIdx.x, reinterpret_cast<uint64_t*>(smem_raw));
 }
 
 // ---------------------------------------------------------------------------
@@ -495,7 +508,7 @@ struct NttBatchTable {
   NttPass pass[kMaxBatchPasses];
 };
 
-template <class F>
+template <class F, bool kShared>
 __global__ void __launch_bounds__(kBatchThreads) k_ntt_batch(F f, const __grid_constant__ NttBatchTable T,
                                                              unsigned long long* next_tile,
                                                              unsigned* done, int* status) {
@@ -537,7 +550,7 @@ __global__ void __launch_bounds__(kBatchThreads) k_ntt_batch(F f, const __grid_c
     __syncthreads();
     if (!s_go) break;
     const int p = s_pass;
-    ntt_tile<F, true>(f, T.pass[p], s_tile - T.tile_start[p], sm);
+    ntt_tile<F, true, kShared>(f, T.pass[p], s_tile - T.tile_start[p], sm);
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) atomicAdd(done + p, 1u);
@@ -762,7 +775,7 @@ static int run_ntt(const F& f, const zkb_field* field, const uint64_t* in, uint6
   const int P = (int)passes.size();
   for (int q = 0; q < P; ++q) {
     const PassLaunch& L = passes[q];
-    auto kern = k_ntt_pass<F>;
+    auto kern = tune_get("ntt.call_products") ? k_ntt_pass<F, true> : k_ntt_pass<F, false>;
     ZKB_TRY(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)L.smem),
                        "NTT shared memory attribute"));
@@ -884,7 +897,7 @@ static int run_ntt_batch(const F& f, const zkb_field* field, const zkb_ntt_job* 
   ZKB_TRY(check_cuda(cudaMemsetAsync(ws, 0, L.off_done + (size_t)kMaxBatchPasses * 4, s),
                      "NTT batch counters"));
   if (np > 0) {
-    auto kern = k_ntt_batch<F>;
+    auto kern = tune_get("ntt.call_products") ? k_ntt_batch<F, true> : k_ntt_batch<F, false>;
     ZKB_TRY(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)smem),
                        "NTT batch shared memory attribute"));
