@@ -59,7 +59,7 @@ COSET = 5
 WORKLOADS = {
     # name: (log2 MSM points, log2 NTT size)
     "large": (22, 24),
-    "small": (18, 20),  # for profiler captures: a few GB on the device
+    "small": (20, 22),  # for profiler captures: inputs above the L2 size, ~2 GB on the device
     "tiny": (10, 10),   # for the CPU tests of the reference arm
 }
 
@@ -348,7 +348,9 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     clk = clocks.summary()
     peaks = _peaks()
     sm_count = torch.cuda.get_device_properties(device).multi_processor_count
-    mhz = clk.get("sm_mhz") or peaks.get("clocks_under_load", {}).get("sm_mhz_median") or peaks.get("sm_max_mhz", 1965.0)
+    # the clock sampled during the timed region; a region too short for a sample
+    # takes the maximum SM clock (never a lower clock, which would inflate frac)
+    mhz = clk.get("sm_mhz") or peaks.get("sm_max_mhz") or 1965.0
     imad_peak_t = sm_count * 64 * mhz * 1e6 / 1e12  # T IMAD/s at the sampled clock
     madds = nonzero_digits(step.sc_uniform_host, step.w)
     acc_count, acc_ms = prof_msm.get("msm_acc_points", (1, float("nan")))
@@ -428,16 +430,23 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
 
 def _profile_traffic(kernel: str, n: int) -> float | None:
     """DRAM bytes per launch of *kernel* from a committed ncu summary (profiles/*.txt lines
-    `traffic <kernel> <points> <bytes>`), scaled to n points; None when not captured yet."""
+    `traffic <kernel> <points> <bytes>`): the capture at exactly n points, else the largest
+    capture scaled to n; None when not captured yet."""
+    found: dict[float, float] = {}
     for f in sorted((ROOT / "profiles").glob("*.txt")):
         for line in f.read_text().splitlines():
             parts = line.split()
             if len(parts) == 4 and parts[0] == "traffic" and parts[1] == kernel:
                 try:
-                    return round(float(parts[3]) * n / float(parts[2]))
+                    found[float(parts[2])] = float(parts[3])
                 except ValueError:
                     continue
-    return None
+    if not found:
+        return None
+    if float(n) in found:
+        return round(found[float(n)])
+    points = max(found)
+    return round(found[points] * n / points)
 
 
 def _run_e2e(args, step: Step, dist, device, log_msm: int, log_ntt: int) -> dict:

@@ -132,6 +132,26 @@ size_t zkb_ntt_batch_workspace_bytes(const zkb_ntt_job* jobs, int count);
 int zkb_ntt_batch(const zkb_field* f, const zkb_ntt_job* jobs, int count, void* workspace,
                   size_t workspace_bytes, int32_t* status, void* stream);
 
+/* The cross-part step of one BN254 Fr NTT of n rows split over `parts` GPUs
+ * (parts = G, a power of 2 in 2..16; G^2 <= n). It has no counterpart in the
+ * reference, which runs on one GPU; it is the step that makes the single
+ * transform of zkb_ntt shard (the four-step decomposition n = G m, m = n / G).
+ * With the input in block layout (part r holds x[r m .. r m + m)), a first
+ * exchange gives part s the rows x[j1 m + s c + i] of every j1 < G (c = m / G),
+ * stored as `in` = (G, c): block j1 from part j1. This call writes `out` =
+ * (G, c), block k1 bound for part k1:
+ *   out[k1][i] = post[k1] w_n^(j2 k1) sum_j1 in[j1][i] w_G^(j1 k1),  j2 = s c + i,
+ * with w^-1 when `invert`, and x[j] pre-scaled by g^j for a forward coset
+ * transform (`coset`: host pointer to g's plain value, or NULL). `post` is a
+ * device array of G Montgomery rows, or NULL for 1: G^-1 for an inverse
+ * transform (times g^-k1 for an inverse coset). After a second exchange part t
+ * holds the rows for k1 = t of every part in order, and zkb_ntt of size m
+ * (inverse ones with coset offset g^G) yields y[t + k2 G] for k2 < m: cyclic
+ * layout. zkgpu/sharded.py drives the whole transform over torch.distributed. */
+int zkb_ntt_cross_step(const zkb_field* f, const uint64_t* in, uint64_t* out, int64_t n, int parts,
+                       int part, int invert, const uint64_t* coset, const uint64_t* post,
+                       void* stream);
+
 /* Replaces the quotient step of the reference's GPU prover,
  * Fr.mul(Fr.sub(Fr.mul(a, b), c), z_inv) (demo/prover_simulation.py:148):
  * out[i] = (a[i] b[i] - c[i]) z over BN254 Fr, in one pass. a, b, c, out are

@@ -918,6 +918,128 @@ static int run_ntt_batch(const F& f, const zkb_field* field, const zkb_ntt_job* 
   return ZKB_OK;
 }
 
+// ---------------------------------------------------------------------------
+// The cross-part step of an NTT split over G parts (one per GPU)
+// ---------------------------------------------------------------------------
+//
+// n = G m, and part r holds the rows x[r m .. r m + m) (block layout). With
+// j = j1 m + j2 (j1 < G, j2 < m) and k = k1 + k2 G:
+//   y[k1 + k2 G] = sum_j2 w_m^(j2 k2) [ w_n^(j2 k1) sum_j1 x[j1 m + j2] w_G^(j1 k1) ].
+// After a first exchange part s holds, for its columns j2 = s c + i (c = m / G),
+// the G rows x[j1 m + j2] of every j1 (input block j1 came from part j1). This
+// step computes, per column, the G-point transform over j1 in registers, the
+// twiddle w_n^(j2 k1) and an optional per-block factor post[k1], and writes
+// output block k1 (bound for part k1). After a second exchange part t holds
+// the bracket for k1 = t and every j2, and an ordinary m-point NTT of it gives
+// y[t + k2 G]: the output is in cyclic layout. An inverse uses w^-1 and
+// post[k1] = G^-1 (times g^-k1 for a coset); a forward coset transform scales
+// x[j] by g^j on the way in.
+
+template <class F, int LG>
+__global__ void __launch_bounds__(128) k_ntt_cross(F f, const uint64_t* in, uint64_t* out,
+                                                    int64_t c, int64_t m, int part, int log_n,
+                                                    int inverse, RootTables rt, ScaleTables st,
+                                                    const uint64_t* post) {
+  constexpr int G = 1 << LG;
+  const uint64_t N = 1ull << rt.log_N;
+  const int shift = rt.log_N - log_n;  // w_n^e = w_N^(e 2^shift)
+  const uint64_t mask = (1ull << rt.s) - 1;
+  auto root = [&](uint32_t r[8], uint64_t e_n) {  // w_n^(+-e_n), e_n < n
+    uint64_t e = e_n << shift;
+    if (inverse && e) e = N - e;
+    uint32_t lo[8], hi[8];
+    fe_load_nc(lo, rt.t_lo + 4 * (e & mask));
+    fe_load_nc(hi, rt.t_hi + 4 * (e >> rt.s));
+    fe_mul(r, lo, hi, f);
+  };
+  // w_G^t for t < G / 2
+  uint32_t wg[G / 2 > 0 ? G / 2 : 1][8];
+#pragma unroll
+  for (int t = 0; t < G / 2; ++t) root(wg[t], (uint64_t)t * (uint64_t)m);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < c; i += stride) {
+    const int64_t j2 = (int64_t)part * c + i;
+    uint32_t a[G][8];
+#pragma unroll
+    for (int j1 = 0; j1 < G; ++j1) {
+      // bit-reversed order for the in-place decimation-in-time transform below
+      const int src = (int)(__brev((unsigned)j1) >> (32 - (LG > 0 ? LG : 1))) & (G - 1);
+      fe_load_nc(a[j1], in + 4 * ((int64_t)src * c + i));
+      if (st.g_lo && !inverse) {
+        const uint64_t j = (uint64_t)src * (uint64_t)m + (uint64_t)j2;
+        const uint64_t gm = (1ull << st.gs) - 1;
+        uint32_t lo[8], hi[8];
+        fe_load_nc(lo, st.g_lo + 4 * (j & gm));
+        fe_load_nc(hi, st.g_hi + 4 * (j >> st.gs));
+        fe_mul(lo, lo, hi, f);
+        fe_mul(a[j1], a[j1], lo, f);
+      }
+    }
+#pragma unroll
+    for (int h = 1; h < G; h <<= 1) {
+#pragma unroll
+      for (int b = 0; b < G; b += 2 * h) {
+#pragma unroll
+        for (int jj = 0; jj < h; ++jj) {
+          uint32_t v[8], u[8];
+          fe_copy(u, a[b + jj]);
+          if (jj) {
+            fe_mul(v, a[b + jj + h], wg[jj * (G / (2 * h))], f);
+          } else {
+            fe_copy(v, a[b + jj + h]);
+          }
+          fe_add(a[b + jj], u, v, f);
+          fe_sub(a[b + jj + h], u, v, f);
+        }
+      }
+    }
+    // twiddle w_n^(j2 k1) by successive powers of w_n^j2, then the block factor
+    uint32_t base[8], tw[8];
+    root(base, (uint64_t)j2);
+    fe_copy(tw, base);
+#pragma unroll
+    for (int k1 = 0; k1 < G; ++k1) {
+      uint32_t x[8];
+      fe_copy(x, a[k1]);
+      if (k1 > 0) {
+        fe_mul(x, x, tw, f);
+        if (k1 + 1 < G) fe_mul(tw, tw, base, f);
+      }
+      if (post) {  // Montgomery row post[k1]
+        uint32_t pf[8];
+        fe_load_nc(pf, post + 4 * k1);
+        fe_mul(x, x, pf, f);
+      }
+      fe_store(out + 4 * ((int64_t)k1 * c + i), x);
+    }
+  }
+}
+
+template <class F>
+static int run_cross(const F& f, const zkb_field* field, const uint64_t* in, uint64_t* out,
+                     int64_t n, int parts, int part, int invert, const uint64_t* coset,
+                     const uint64_t* post, cudaStream_t s) {
+  const int log_n = ilog2(n);
+  int lg = 0;
+  while ((1 << lg) < parts) ++lg;
+  int device = 0;
+  ZKB_TRY(check_cuda(cudaGetDevice(&device), "cudaGetDevice"));
+  RootTables rt;
+  ScaleTables st;
+  // forward coset: the scaling tables g^j of size n (inverse transforms take post[])
+  ZKB_TRY(lookup_tables(f, table_key(field, nullptr, log_n, device), n, log_n, 0,
+                        invert ? nullptr : coset, rt, st, s));
+  const int64_t m = n >> lg, c = m >> lg;
+  const unsigned grid = grid_for(c, 128);
+  switch (lg) {
+    case 1: k_ntt_cross<F, 1><<<grid, 128, 0, s>>>(f, in, out, c, m, part, log_n, invert, rt, st, post); break;
+    case 2: k_ntt_cross<F, 2><<<grid, 128, 0, s>>>(f, in, out, c, m, part, log_n, invert, rt, st, post); break;
+    case 3: k_ntt_cross<F, 3><<<grid, 128, 0, s>>>(f, in, out, c, m, part, log_n, invert, rt, st, post); break;
+    default: k_ntt_cross<F, 4><<<grid, 128, 0, s>>>(f, in, out, c, m, part, log_n, invert, rt, st, post); break;
+  }
+  return check_launch("NTT cross-part step");
+}
+
 }  // namespace zkb
 
 using namespace zkb;
@@ -951,6 +1073,31 @@ int zkb_ntt(const zkb_field* f, const uint64_t* in, uint64_t* out, int64_t n, in
   return with_field(f, [&](auto fp) {
     return run_ntt(fp, f, in, out, n, invert, omega, coset, workspace, workspace_bytes, s);
   });
+}
+
+int zkb_ntt_cross_step(const zkb_field* f, const uint64_t* in, uint64_t* out, int64_t n, int parts,
+                       int part, int invert, const uint64_t* coset, const uint64_t* post,
+                       void* stream) {
+  set_error("%s", "");
+  ZKB_TRY(check_field(f));
+  if (f->kind != ZKB_FIELD_BN254_FR) {
+    return fail(ZKB_EINVAL, "split NTTs use BN254 Fr's built-in roots of unity");
+  }
+  if (parts < 2 || parts > 16 || (parts & (parts - 1))) {
+    return fail(ZKB_EINVAL, "parts must be a power of 2 in 2..16, got %d", parts);
+  }
+  if (part < 0 || part >= parts) return fail(ZKB_EINVAL, "part %d out of 0..%d", part, parts - 1);
+  if (n < (int64_t)parts * parts || (n & (n - 1)) || n > (1ll << kMaxLogN)) {
+    return fail(ZKB_EINVAL, "NTT length must be a power of 2 in parts^2..2^28, got %lld",
+                (long long)n);
+  }
+  if (!in || !out) return fail(ZKB_EINVAL, "null buffer");
+  if (in == out) return fail(ZKB_EINVAL, "output must not alias the input");
+  ZKB_TRY(check_align(in, 16, "in"));
+  ZKB_TRY(check_align(out, 16, "out"));
+  ZKB_TRY(check_align(post, 16, "post"));
+  cudaStream_t s = as_stream(stream);
+  return run_cross(FrP{}, f, in, out, n, parts, part, invert, coset, post, s);
 }
 
 size_t zkb_ntt_batch_workspace_bytes(const zkb_ntt_job* jobs, int count) {

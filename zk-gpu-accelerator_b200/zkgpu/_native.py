@@ -99,6 +99,11 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "zkb_ntt_batch_workspace_bytes": (ctypes.c_size_t, [_nttjobp, ctypes.c_int]),
     "zkb_ntt_batch": (ctypes.c_int, [_fp, _nttjobp, ctypes.c_int, _vp, ctypes.c_size_t, _vp, _vp]),
     "zkb_quotient_pointwise": (ctypes.c_int, [_u64p, _u64p, _u64p, _u64p, _u64p, _i64, _vp]),
+    "zkb_ntt_cross_step": (
+        ctypes.c_int,
+        [_fp, _u64p, _u64p, _i64, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64),
+         _u64p, _vp],
+    ),
     "zkb_g1_add": (ctypes.c_int, [_u64p, _i64, _u64p, _i64, _u64p, _i64, _vp]),
     "zkb_g1_add_affine": (ctypes.c_int, [_u64p, _i64, _u64p, _i64, _u64p, _i64, _vp]),
     "zkb_g1_double": (ctypes.c_int, [_u64p, _u64p, _i64, _vp]),
