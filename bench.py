@@ -297,6 +297,16 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     device = torch.device("cuda", local_rank)
     dist = init_dist(world, "nccl")
     log_msm, log_ntt = WORKLOADS[args.workload]
+    tuned = None
+    if args.tune:
+        from zkgpu import autotune
+
+        t0 = time.perf_counter()
+        table = autotune.autotune(range(10, log_msm + 1), range(10, log_ntt + 1))
+        tuned = {"seconds": round(time.perf_counter() - t0, 1), "device": table["device"],
+                 "msm_window": {int(k): v["window"] for k, v in table["msm"].items()},
+                 "ntt_radix_tile_threads": {int(k): [v["max_log_radix"], v["cta_log_elems"], v["threads"]]
+                                            for k, v in table["ntt"].items()}}
     step = Step(log_msm, log_ntt, seed=10 + 100 * rank)
 
     def one_step() -> None:
@@ -422,6 +432,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         "clocks": clk,
         "e2e": e2e,
         "cpu_baseline": cpu,
+        "autotune": tuned,
         "batched": batched,
         "served": served,
     }
@@ -747,6 +758,8 @@ def main() -> None:
     ap.add_argument("--skip-cpu-baseline", action="store_true")
     ap.add_argument("--skip-batched", action="store_true", help="skip the batched form (64 NTTs + 32 MSMs)")
     ap.add_argument("--skip-served", action="store_true", help="skip the served form (Poisson job stream)")
+    ap.add_argument("--tune", action="store_true",
+                    help="measure (or load from the cache) per-size MSM windows and NTT shapes first")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3  # at least three untimed steps

@@ -274,6 +274,19 @@ int zkb_msm_batch(const zkb_msm_job* jobs, int count, void* workspace, size_t wo
 int zkb_tune_set(const char* key, int value);
 int zkb_tune_get(const char* key, int* value);
 
+/* Per-size tuning tables, one entry per log2 problem size (0..32): what an
+ * autotuner measured best (zkgpu/autotune.py fills and caches them). It
+ * replaces the reference's addition-count window model
+ * (pippenger_window_size, zkgpu/msm.py:112-121) with measured choices.
+ * Tables: "msm.window" (1..20; the default window of an MSM whose point count
+ * rounds up to 2^log_n), "ntt.max_log_radix" (8..12), "ntt.cta_log_elems"
+ * (9..12), "ntt.threads" (64..512) for an NTT of 2^log_n rows. value = 0
+ * clears an entry. An entry takes precedence over the process-wide knob of
+ * the same name. Tables are read when a call plans its work: change them
+ * between a workspace-size query and the call it sizes and the two disagree. */
+int zkb_tune_set_sized(const char* key, int log_n, int value);
+int zkb_tune_get_sized(const char* key, int log_n, int* value);
+
 /* Number of this library's own kernels launched so far in this process
  * (sorting kernels of the CUB library are not counted). */
 uint64_t zkb_launch_count(void);

@@ -308,3 +308,41 @@ def test_product_never_imports_the_oracle():
     for src in pkg.glob("*.py"):
         text = src.read_text()
         assert "import oracle" not in text and "from oracle" not in text, src.name
+
+
+# ------------------------------------------------------------------
+# Per-size tuning tables and the autotuner's cache (no GPU needed)
+# ------------------------------------------------------------------
+
+
+def test_per_size_tables_drive_the_plans(tmp_path):
+    from zkgpu import autotune
+
+    lib = _native.lib()
+    with pytest.raises(ValueError, match="unknown per-size"):
+        _native.tune_set_sized("msm.bogus", 10, 3)
+    with pytest.raises(ValueError, match="1..20"):
+        _native.tune_set_sized("msm.window", 10, 21)
+    with pytest.raises(ValueError, match="0..32"):
+        _native.tune_set_sized("msm.window", 40, 3)
+    model = lib.zkb_msm_default_window(3000)
+    try:
+        _native.tune_set_sized("msm.window", 12, 7)  # 3000 points round up to 2^12
+        assert lib.zkb_msm_default_window(3000) == 7
+        assert lib.zkb_msm_default_window(5000) == lib.zkb_msm_default_window(8192)  # the 2^13 entry: none
+        _native.tune_set_sized("ntt.max_log_radix", 9, 8)  # 2^9 rows in two passes
+        assert lib.zkb_ntt_workspace_bytes(512) == 512 * 32
+        assert lib.zkb_ntt_workspace_bytes(256) == 0
+        table = {"device": "test-gpu", "msm": {12: {"window": 9}},
+                 "ntt": {20: {"max_log_radix": 10, "cta_log_elems": 11, "threads": 256}}}
+        path = autotune.save(table, tmp_path / "tune.json")
+        back = autotune.load(path, key="test-gpu")
+        assert back["msm"]["12"]["window"] == 9 and back["ntt"]["20"]["threads"] == 256
+        assert autotune.load(path, key="other-gpu") is None
+        autotune.apply(back)
+        assert _native.tune_get_sized("msm.window", 12) == 9
+        assert _native.tune_get_sized("ntt.cta_log_elems", 20) == 11
+    finally:
+        autotune.clear()
+    assert lib.zkb_msm_default_window(3000) == model
+    assert lib.zkb_ntt_workspace_bytes(512) == 0

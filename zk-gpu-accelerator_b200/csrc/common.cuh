@@ -40,6 +40,11 @@ void count_launch();
 // Tuning knobs read when a call plans its work (zkb_tune_set / zkb_tune_get).
 int tune_get(const char* key);
 
+// Per-size tuning tables (zkb_tune_set_sized): the entry for log2 size log_n,
+// or 0 when the table has none.
+constexpr int kMaxSizedLog = 32;
+int tune_get_sized(const char* key, int log_n);
+
 inline int check_launch(const char* what) {
   count_launch();
   return check_cuda(cudaGetLastError(), what);

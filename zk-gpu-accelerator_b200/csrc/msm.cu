@@ -585,6 +585,10 @@ int default_window(int64_t n) {
   // multiplications: 10 per mixed addition, about 42 per bucket in the
   // running sums.
   if (n <= 1) return 1;
+  int log_n = 0;
+  while ((1ll << log_n) < n) ++log_n;
+  const int tuned = tune_get_sized("msm.window", log_n);  // a measured table's entry
+  if (tuned > 0) return tuned;
   int best_w = 1;
   double best = 1e300;
   for (int w = 1; w <= 16; ++w) {

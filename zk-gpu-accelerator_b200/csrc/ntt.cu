@@ -574,8 +574,10 @@ static int ilog2(int64_t n) {
 // in two: one pass would be a single CTA on one SM, while two passes of
 // 2^5..2^6-point sub-transforms spread it over 32-64 CTAs (2^12 rows: 0.048
 // ms instead of 0.11 ms on a B200).
+// A per-size table entry (an autotuner's) takes precedence over the knob.
 static std::vector<int> plan_radices(int log_n) {
-  const int max_r = tune_get("ntt.max_log_radix");
+  const int tuned = tune_get_sized("ntt.max_log_radix", log_n);
+  const int max_r = tuned > 0 ? tuned : tune_get("ntt.max_log_radix");
   int P = (log_n + max_r - 1) / max_r;
   if (P > 3) P = 3;
   if (P < (log_n + kMaxLogR - 1) / kMaxLogR) P = (log_n + kMaxLogR - 1) / kMaxLogR;
@@ -691,12 +693,16 @@ static void plan_passes(int64_t n, int log_n, int invert, const RootTables& rt,
   // when that gives at least 16 CTAs per SM (2^24 rows and up on a B200),
   // else 1024-row tiles of 256 threads, several per SM, which measured faster
   // from 2^12 to 2^22 rows.
+  // A per-size table entry takes precedence over the knob, which takes
+  // precedence over the rule.
   if (cta_log == 0) {
-    cta_log = tune_get("ntt.cta_log_elems");
+    cta_log = tune_get_sized("ntt.cta_log_elems", log_n);
+    if (cta_log < 9) cta_log = tune_get("ntt.cta_log_elems");
     if (cta_log < 9) cta_log = (n >> kMaxLogR) >= 16 * sms ? kMaxLogR : 10;
   }
   if (threads == 0) {
-    threads = tune_get("ntt.threads");
+    threads = tune_get_sized("ntt.threads", log_n);
+    if (threads < 64) threads = tune_get("ntt.threads");
     if (threads < 64) threads = cta_log >= kMaxLogR ? 512 : 256;
   }
   passes.clear();

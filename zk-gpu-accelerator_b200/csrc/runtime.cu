@@ -45,6 +45,35 @@ int tune_get(const char* key) {
   return k ? k->value : 0;
 }
 
+// ---- per-size tuning tables ---------------------------------------------------
+// Choices that depend on the problem size, set per log2 size (an autotuner's
+// measured table); 0 = no entry, the planner's own rule applies.
+struct SizedKnob {
+  const char* name;
+  int lo, hi;
+  int value[kMaxSizedLog + 1];
+};
+static SizedKnob g_sized[] = {
+    {"msm.window", 1, 20, {}},          // MSM window for ceil(log2 n) = log
+    {"ntt.max_log_radix", 8, 12, {}},   // largest pass radix for an NTT of 2^log rows
+    {"ntt.cta_log_elems", 9, 12, {}},   // rows per NTT block
+    {"ntt.threads", 64, 512, {}},       // threads per NTT block
+};
+
+static SizedKnob* find_sized(const char* key) {
+  if (!key) return nullptr;
+  for (auto& k : g_sized)
+    if (std::strcmp(k.name, key) == 0) return &k;
+  return nullptr;
+}
+
+int tune_get_sized(const char* key, int log_n) {
+  if (log_n < 0 || log_n > kMaxSizedLog) return 0;
+  std::lock_guard<std::mutex> lock(g_knob_mutex);
+  SizedKnob* k = find_sized(key);
+  return k ? k->value[log_n] : 0;
+}
+
 void set_error(const char* fmt, ...) {
   va_list ap;
   va_start(ap, fmt);
@@ -158,6 +187,34 @@ int zkb_tune_set(const char* key, int value) {
     return zkb::fail(ZKB_EINVAL, "%s must be in %d..%d, got %d", k->name, k->lo, k->hi, value);
   }
   k->value = value;
+  return ZKB_OK;
+}
+
+int zkb_tune_set_sized(const char* key, int log_n, int value) {
+  zkb::set_error("%s", "");
+  std::lock_guard<std::mutex> lock(zkb::g_knob_mutex);
+  zkb::SizedKnob* k = zkb::find_sized(key);
+  if (!k) return zkb::fail(ZKB_EINVAL, "unknown per-size tuning table '%s'", key ? key : "(null)");
+  if (log_n < 0 || log_n > zkb::kMaxSizedLog) {
+    return zkb::fail(ZKB_EINVAL, "log2 size must be in 0..%d, got %d", zkb::kMaxSizedLog, log_n);
+  }
+  if (value != 0 && (value < k->lo || value > k->hi)) {
+    return zkb::fail(ZKB_EINVAL, "%s must be 0 (no entry) or in %d..%d, got %d", k->name, k->lo, k->hi,
+                     value);
+  }
+  k->value[log_n] = value;
+  return ZKB_OK;
+}
+
+int zkb_tune_get_sized(const char* key, int log_n, int* value) {
+  zkb::set_error("%s", "");
+  std::lock_guard<std::mutex> lock(zkb::g_knob_mutex);
+  zkb::SizedKnob* k = zkb::find_sized(key);
+  if (!k || !value) return zkb::fail(ZKB_EINVAL, "unknown per-size tuning table '%s'", key ? key : "(null)");
+  if (log_n < 0 || log_n > zkb::kMaxSizedLog) {
+    return zkb::fail(ZKB_EINVAL, "log2 size must be in 0..%d, got %d", zkb::kMaxSizedLog, log_n);
+  }
+  *value = k->value[log_n];
   return ZKB_OK;
 }
 

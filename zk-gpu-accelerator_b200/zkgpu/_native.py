@@ -120,6 +120,8 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "zkb_launch_count": (ctypes.c_uint64, []),
     "zkb_tune_set": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int]),
     "zkb_tune_get": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)]),
+    "zkb_tune_set_sized": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int]),
+    "zkb_tune_get_sized": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     "zkb_profile_enable": (None, [ctypes.c_int]),
     "zkb_profile_report": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_size_t]),
 }
@@ -223,6 +225,17 @@ def tune_set(key: str, value: int) -> None:
 def tune_get(key: str) -> int:
     v = ctypes.c_int(0)
     check(lib().zkb_tune_get(key.encode(), ctypes.byref(v)), "zkb_tune_get")
+    return v.value
+
+
+def tune_set_sized(key: str, log_n: int, value: int) -> None:
+    """Set (value > 0) or clear (0) one entry of a per-size tuning table (zkb_tune_set_sized)."""
+    check(lib().zkb_tune_set_sized(key.encode(), int(log_n), int(value)), "zkb_tune_set_sized")
+
+
+def tune_get_sized(key: str, log_n: int) -> int:
+    v = ctypes.c_int(0)
+    check(lib().zkb_tune_get_sized(key.encode(), int(log_n), ctypes.byref(v)), "zkb_tune_get_sized")
     return v.value
 
 
