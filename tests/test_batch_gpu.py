@@ -159,3 +159,29 @@ def test_captured_batch_plan_replays_exactly(base_set):
     assert bool((plan.ntt_outputs[1] == BN254_FR.ntt(ntt_in[1], invert=True, coset=5)).all())
     assert plan.msm_points_out()[0] == msm_pippenger_rows(base_set[: 1 << 12], msm_sc[0], check_points=False)
     assert plan.launches_per_run > 0
+
+
+def test_concurrent_plan_equals_the_sequential_plan_and_replays(base_set):
+    """MSM batch on a high-priority stream, transforms on a low-priority one: same rows and
+    points as the plain order, eagerly and from a captured graph."""
+    import torch
+
+    x = _rows_fr(800, 1 << 16)
+    sc = [torch.from_numpy(wl.uniform_fr(801, 1 << 15)).cuda(), torch.from_numpy(wl.skewed_scalars(802, 1 << 16)).cuda()]
+    jobs = dict(ntt_jobs=[(x, False, None), (x, True, 5)],
+                msm_jobs=[(base_set[: 1 << 15], sc[0], None), (base_set, sc[1], None)])
+    seq = batch.BatchPlan(**jobs)
+    seq.run()
+    conc = batch.BatchPlan(**jobs, concurrent=True)
+    conc.run()
+    torch.cuda.synchronize()
+    assert all(bool((a == b).all()) for a, b in zip(seq.ntt_outputs, conc.ntt_outputs, strict=True))
+    assert seq.msm_points_out() == conc.msm_points_out()
+    conc.capture()
+    for y in conc.ntt_outputs:
+        y.zero_()
+    conc.msm_results.zero_()
+    conc.replay()
+    torch.cuda.synchronize()
+    assert all(bool((a == b).all()) for a, b in zip(seq.ntt_outputs, conc.ntt_outputs, strict=True))
+    assert seq.msm_points_out() == conc.msm_points_out()

@@ -170,12 +170,27 @@ class BatchPlan:
 
     ntt_jobs : [(rows, invert, coset)] with rows (n, 4) Montgomery, device
     msm_jobs : [(points, scalars, window_size)] device tensors
+    concurrent : run the MSM batch on a high-priority stream and the transforms,
+                 one pass launch at a time (zkb_ntt per job), on a low-priority
+                 stream beside it. The block scheduler then hands SMs to NTT
+                 blocks whenever the MSM kernels have none waiting: during the
+                 memory-bound sort, the tail of every wave and the
+                 latency-bound bucket reduction and final combination, so
+                 those overlap the transforms. run() still returns with all
+                 the work ordered on the current stream.
     """
 
     def __init__(self, ntt_jobs: Sequence[tuple[Any, bool, int | None]] = (),
-                 msm_jobs: Sequence[tuple[Any, Any, int | None]] = ()) -> None:
+                 msm_jobs: Sequence[tuple[Any, Any, int | None]] = (), concurrent: bool = False) -> None:
         torch = _native.require_cuda()
         self._torch = torch
+        self._concurrent = concurrent
+        if concurrent:
+            lo, hi = torch.cuda.Stream.priority_range()
+            self._hi = torch.cuda.Stream(priority=hi)
+            self._lo = torch.cuda.Stream(priority=lo)
+            self._ntt_single_ws = [_native.workspace(_native.lib().zkb_ntt_workspace_bytes(int(j[0].shape[0])))
+                                   for j in ntt_jobs]
         lib = _native.lib()
         xs = [j[0] for j in ntt_jobs]
         inv, cos = _check_ntt_inputs(xs, [j[1] for j in ntt_jobs], [j[2] for j in ntt_jobs])
@@ -204,16 +219,33 @@ class BatchPlan:
 
     def run(self) -> None:
         """Queue every job on the current stream (asynchronous)."""
+        torch = self._torch
         lib = _native.lib()
-        stream = _native.stream_ptr()
+        main = torch.cuda.current_stream()
         before = int(lib.zkb_launch_count())
-        if self._ntt_count:
+        split = self._concurrent and self._ntt_count and self._msm_count
+        ntt_stream, msm_stream = (self._lo, self._hi) if split else (main, main)
+        if split:
+            self._lo.wait_stream(main)
+            self._hi.wait_stream(main)
+            f = BN254_FR._field()
+            for k in range(self._ntt_count):
+                j = self._ntt[k]
+                g = _native.u64_array(list(j.coset)) if j.has_coset else None
+                ws = self._ntt_single_ws[k]
+                _native.check(lib.zkb_ntt(ctypes.byref(f), j.input, j.out, j.n, j.invert, None, g,
+                                          _native.ptr(ws), ws.numel(), int(ntt_stream.cuda_stream)), "zkb_ntt")
+        elif self._ntt_count:
             _native.check(lib.zkb_ntt_batch(ctypes.byref(BN254_FR._field()), self._ntt, self._ntt_count,
                                             _native.ptr(self._ntt_ws), self._ntt_ws_bytes,
-                                            _native.ptr(self.status), stream), "zkb_ntt_batch")
+                                            _native.ptr(self.status), int(ntt_stream.cuda_stream)),
+                          "zkb_ntt_batch")
         if self._msm_count:
             _native.check(lib.zkb_msm_batch(self._msm, self._msm_count, _native.ptr(self._msm_ws),
-                                            self._msm_ws_bytes, stream), "zkb_msm_batch")
+                                            self._msm_ws_bytes, int(msm_stream.cuda_stream)), "zkb_msm_batch")
+        if split:
+            main.wait_stream(self._lo)
+            main.wait_stream(self._hi)
         self.launches_per_run = int(lib.zkb_launch_count()) - before
 
     def capture(self) -> None:
