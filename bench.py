@@ -644,6 +644,11 @@ def run_served(n_jobs: int = 2000, rate: float = 200.0, log_max: int = 20, seed:
     wall = time.perf_counter() - t0
     s = summarize(recs, wall)
     plain_jobs_s = len(sample) / plain_s
+    # capacity: the first 200 jobs all queued at once (closed loop)
+    cap = Server(bases, budget)
+    t0 = time.perf_counter()
+    cap_recs = cap.run(reqs[:200], [0.0] * min(200, n_jobs))
+    cap_s = summarize(cap_recs, time.perf_counter() - t0)
     return {
         "workload": f"{n_jobs} Groth16-shaped jobs, Poisson {rate:g}/s, m = 2^U{{12..{log_max}}}, 7 NTTs + "
                     f"4 G1 MSMs each, resident 2^{log_max} base set (seed {seed})",
@@ -651,6 +656,9 @@ def run_served(n_jobs: int = 2000, rate: float = 200.0, log_max: int = 20, seed:
         "p50_ms": round(s["p50_ms"], 2), "p90_ms": round(s["p90_ms"], 2), "p99_ms": round(s["p99_ms"], 2),
         "max_ms": round(s["max_ms"], 2), "plain_jobs_per_s": round(plain_jobs_s, 1),
         "speedup_vs_plain": round(s["jobs_per_s"] / plain_jobs_s, 3),
+        "capacity_jobs_per_s": round(cap_s["jobs_per_s"], 1),
+        "capacity_vs_plain": round(cap_s["jobs_per_s"] / plain_jobs_s, 3),
+        "capacity": "the first 200 jobs queued at once (closed loop), same server",
         "plain": f"the first {len(sample)} jobs one at a time (one call per NTT / MSM, synchronised per job)",
         "ticks": srv.ticks, "gpu_launches": srv.launches, "hbm_budget_bytes": budget,
         "latency": "arrival (host clock) to the device-side completion of the job's last MSM batch",

@@ -11,11 +11,17 @@ The service
 - advances every job in flight by one stage per tick, and launches each
   tick's work for ALL jobs together: the tick's transforms of every job in
   one persistent NTT launch (zkb_ntt_batch, 64 per launch), the fused
-  quotient steps, and the MSMs in MSM batches (zkb_msm_batch) on MSM
-  streams: the A, B and L MSMs of the jobs admitted in the tick (they need
-  only the witness) and the H MSMs of the jobs whose h is ready. The MSM
-  batches rotate over several streams, so they overlap the transforms and
-  each other's latency-bound tails;
+  quotient steps;
+- queues the MSMs: the A, B and L MSMs of a job when it is admitted (they
+  need only the witness), its H MSM when h is ready. Each of two
+  high-priority MSM streams takes the queued MSMs, first come first served
+  up to 2^22 points, as one batch (zkb_msm_batch) whenever its previous
+  batch has finished: batches grow with the load and share one sort, bucket
+  pass and tail; one batch's latency-bound tail overlaps the other stream's
+  accumulation; the ticks' transforms fill the SMs the MSMs leave idle.
+  (Measured at 200 jobs/s: high-priority MSMs with the 2^22 cap gave p99
+  159 ms; the reverse priorities, larger caps or taking the whole queue,
+  0.6-1.4 s);
 - admits new jobs at every tick, while others are on the GPU: continuous
   batching, not a queue in front of one-at-a-time launches;
 - reports each job's latency (arrival to the device-side completion of its
@@ -167,19 +173,33 @@ class Server:
     bases       : (N, 2, 4) Montgomery affine rows, resident (the SRS stand-in)
     hbm_budget  : device bytes the jobs in flight may hold (buffers + workspaces)
     max_ticks_ahead : ticks queued on the device before the host waits
+    max_batch_points : an MSM stream takes queued MSMs first come, first served
+                  up to this many points per batch (a bigger group still goes alone)
+    msm_priority / tick_priority : "high", "normal" or "low" stream priority of
+                  the MSM batches and of the ticks' transforms (the block
+                  scheduler serves waiting blocks of higher-priority streams
+                  first)
     """
 
-    def __init__(self, bases: Any, hbm_budget: int, max_ticks_ahead: int = 2, msm_streams: int = 4) -> None:
+    def __init__(self, bases: Any, hbm_budget: int, max_ticks_ahead: int = 2, msm_streams: int = 2,
+                 msm_priority: str = "high", tick_priority: str = "normal",
+                 max_batch_points: int = 1 << 22) -> None:
         torch = _native.require_cuda()
         self.torch = torch
         self.bases = bases
         self.sched = Scheduler(hbm_budget)
         self.max_ticks_ahead = max_ticks_ahead
-        self.main = torch.cuda.current_stream()
-        # MSM batches rotate over several streams, so that one batch's latency-bound tail
-        # (bucket reduction, final combination) overlaps the next batch's accumulation
-        self.msm_streams = [torch.cuda.Stream() for _ in range(max(1, msm_streams))]
-        self.next_msm_stream = 0
+        lo, hi = torch.cuda.Stream.priority_range()
+        level = {"high": hi, "normal": 0, "low": lo}
+        self.main = torch.cuda.Stream(priority=level[tick_priority])
+        # MSM streams pull the pending MSM work whenever their last batch is done; two let
+        # one batch's latency-bound tail (bucket reduction, final combination) overlap the
+        # next batch's accumulation
+        self.msm_streams = [torch.cuda.Stream(priority=level[msm_priority]) for _ in range(max(1, msm_streams))]
+        self.msm_last: list[Any] = [None] * len(self.msm_streams)
+        self.pending_msm: list[tuple[list, list[int], Any]] = []
+        self.msm_batches = 0
+        self.max_batch_points = max_batch_points
         self.jobs: dict[int, ProofJob] = {}
         self.records: dict[int, JobRecord] = {}
         self.pending: dict[int, ProofRequest] = {}
@@ -219,29 +239,31 @@ class Server:
         torch.cuda.synchronize()
         self.start_event = torch.cuda.Event(enable_timing=True)
         self.start_event.record(self.main)
-        t0 = clock()
-        while not self.sched.idle():
-            now = clock() - t0
-            admitted = self.sched.admit(now)
-            for job_id in admitted:
-                self.jobs[job_id] = ProofJob(self.pending.pop(job_id), self.bases, job_id)
-                self.records[job_id].admitted_s = now
-                self.outstanding[job_id] = 0
-            tick = self.sched.next_tick(admitted)
-            if not tick.empty():
-                self._launch(tick)
-            self._collect(block=False)
-            if tick.empty():
-                head_waits = bool(self.sched.queue) and self.sched.queue[0][2] > clock() - t0
-                if self.msm_done and not head_waits:
-                    # nothing to launch until a job finishes (or frees budget)
-                    self._collect(block=True)
-                elif head_waits:
-                    wait = self.sched.queue[0][2] - (clock() - t0)
-                    time.sleep(max(0.0, min(wait, 0.0005 if self.msm_done else 0.002)))
-            while len(self.tick_events) > self.max_ticks_ahead:
-                self.tick_events.popleft().synchronize()
+        with torch.cuda.stream(self.main):  # job buffers, uploads and ticks on the tick stream
+            t0 = clock()
+            while not self.sched.idle():
+                now = clock() - t0
+                admitted = self.sched.admit(now)
+                for job_id in admitted:
+                    self.jobs[job_id] = ProofJob(self.pending.pop(job_id), self.bases, job_id)
+                    self.records[job_id].admitted_s = now
+                    self.outstanding[job_id] = 0
+                tick = self.sched.next_tick(admitted)
+                if not tick.empty():
+                    self._launch(tick)
+                self._dispatch_msm()
                 self._collect(block=False)
+                if tick.empty():
+                    head_waits = bool(self.sched.queue) and self.sched.queue[0][2] > clock() - t0
+                    if self.msm_done and not head_waits:
+                        # nothing to launch until a job finishes (or frees budget)
+                        self._collect(block=True)
+                    elif head_waits:
+                        wait = self.sched.queue[0][2] - (clock() - t0)
+                        time.sleep(max(0.0, min(wait, 0.0005 if self.msm_done else 0.002)))
+                while len(self.tick_events) > self.max_ticks_ahead:
+                    self.tick_events.popleft().synchronize()
+                    self._collect(block=False)
         torch.cuda.synchronize()
         return [self.records[k] for k in range(len(requests))]
 
@@ -265,25 +287,52 @@ class Server:
             self.sched.finish(job_id)
             self.jobs.pop(job_id)
 
-    def _msm_batch(self, entries: list[tuple[int, int, int, int]], ids: list[int], after: Any) -> None:
-        torch = self.torch
-        lib = _native.lib()
-        jobs = (_native.ZkbMsmJob * len(entries))()
-        for j, (pts, sc, n, res) in enumerate(entries):
-            jobs[j].points, jobs[j].scalars, jobs[j].n, jobs[j].result = pts, sc, n, res
-        stream = self.msm_streams[self.next_msm_stream]
-        self.next_msm_stream = (self.next_msm_stream + 1) % len(self.msm_streams)
-        stream.wait_event(after)
-        with torch.cuda.stream(stream):
-            ws_bytes = int(lib.zkb_msm_batch_workspace_bytes(jobs, len(entries)))
-            ws = _native.workspace(ws_bytes)
-            _native.check(lib.zkb_msm_batch(jobs, len(entries), _native.ptr(ws), ws_bytes,
-                                            _native.stream_ptr()), "zkb_msm_batch")
-            done = torch.cuda.Event(enable_timing=True)
-            done.record(stream)
-        self.msm_done.append((done, list(ids)))
+    def _queue_msm(self, entries: list[tuple[int, int, int, int]], ids: list[int], after: Any) -> None:
+        """MSM work becomes pending; an idle MSM stream takes all pending work at once."""
+        self.pending_msm.append((entries, list(ids), after))
         for job_id in ids:
             self.outstanding[job_id] += 1
+
+    def _dispatch_msm(self) -> None:
+        """Launch pending MSMs as one batch on each MSM stream whose last batch has
+        finished: batches grow with the load (up to max_batch_points), so their
+        latency-bound tails are shared."""
+        torch = self.torch
+        lib = _native.lib()
+        for k, stream in enumerate(self.msm_streams):
+            if not self.pending_msm:
+                return
+            last = self.msm_last[k]
+            if last is not None and not last.query():
+                continue
+            # first come, first served, up to max_batch_points points (at least one group)
+            take, points = 0, 0
+            while take < len(self.pending_msm):
+                n = sum(e[2] for e in self.pending_msm[take][0])
+                if take and points + n > self.max_batch_points:
+                    break
+                points += n
+                take += 1
+            work, self.pending_msm = self.pending_msm[:take], self.pending_msm[take:]
+            entries = [e for w in work for e in w[0]]
+            ids = [j for w in work for j in w[1]]
+            jobs = (_native.ZkbMsmJob * len(entries))()
+            for j, (pts, sc, n, res) in enumerate(entries):
+                jobs[j].points, jobs[j].scalars, jobs[j].n, jobs[j].result = pts, sc, n, res
+            for w in work:
+                stream.wait_event(w[2])  # the witness / h these MSMs read is written
+            before = int(lib.zkb_launch_count())
+            with torch.cuda.stream(stream):
+                ws_bytes = int(lib.zkb_msm_batch_workspace_bytes(jobs, len(entries)))
+                ws = _native.workspace(ws_bytes)
+                _native.check(lib.zkb_msm_batch(jobs, len(entries), _native.ptr(ws), ws_bytes,
+                                                _native.stream_ptr()), "zkb_msm_batch")
+                done = torch.cuda.Event(enable_timing=True)
+                done.record(stream)
+            self.launches += int(lib.zkb_launch_count()) - before
+            self.msm_last[k] = done
+            self.msm_done.append((done, ids))
+            self.msm_batches += 1
 
     def _launch(self, tick: Tick) -> None:
         torch = self.torch
@@ -325,11 +374,11 @@ class Server:
         self.prev_tick_event = tick_event
         if tick.admitted:
             # A, B and L need only the witness: they start at admission, beside the quotient
-            self._msm_batch([e for j in tick.admitted for e in self.jobs[j].msm_entries()[:3]],
+            self._queue_msm([e for j in tick.admitted for e in self.jobs[j].msm_entries()[:3]],
                             tick.admitted, upload_event)
         if tick.msm:
             # H needs h, written by the previous tick
-            self._msm_batch([self.jobs[j].msm_entries()[3] for j in tick.msm], tick.msm, prev_event)
+            self._queue_msm([self.jobs[j].msm_entries()[3] for j in tick.msm], tick.msm, prev_event)
         self.ticks += 1
         self.launches += int(lib.zkb_launch_count()) - before
 
