@@ -278,6 +278,30 @@ static void scale_range(void* vctx, int64_t lo, int64_t hi) {
   }
 }
 
+typedef struct {
+  const uint64_t* in;
+  uint64_t* out;
+  int log_n;
+  const uint64_t* g_lo; /* forward coset: out[bitrev(i)] = in[i] g^i, else plain copy */
+  const uint64_t* g_hi;
+  int gs;
+} bitrev_ctx;
+
+static void bitrev_range(void* vctx, int64_t lo, int64_t hi) {
+  bitrev_ctx* c = (bitrev_ctx*)vctx;
+  for (int64_t i = lo; i < hi; ++i) {
+    int64_t r = 0;
+    for (int b = 0; b < c->log_n; ++b) r |= ((i >> b) & 1) << (c->log_n - 1 - b);
+    if (c->g_lo) {
+      uint64_t g[4];
+      fmul(g, c->g_lo + 4 * (i & ((1ll << c->gs) - 1)), c->g_hi + 4 * (i >> c->gs), &FR);
+      fmul(c->out + 4 * r, c->in + 4 * i, g, &FR);
+    } else {
+      memcpy(c->out + 4 * r, c->in + 4 * i, 32);
+    }
+  }
+}
+
 /* tab[i] = base^i for i < count (Montgomery) */
 static void power_table(uint64_t* tab, const uint64_t base[4], int64_t count) {
   if (count <= 0) return;
@@ -296,12 +320,6 @@ int zo_ntt(const uint64_t* in, uint64_t* out, int64_t n, int invert, const uint6
   if (n <= 0 || (n & (n - 1)) || n > (1ll << 28)) return -1;
   int log_n = 0;
   while ((1ll << log_n) < n) ++log_n;
-  /* bit-reversed copy (zkgpu/ntt.py:132-141) */
-  for (int64_t i = 0; i < n; ++i) {
-    int64_t r = 0;
-    for (int b = 0; b < log_n; ++b) r |= ((i >> b) & 1) << (log_n - 1 - b);
-    memcpy(out + 4 * r, in + 4 * i, 32);
-  }
   uint64_t g_m[4], t[4];
   uint64_t *g_lo = NULL, *g_hi = NULL;
   int gs = (log_n + 1) / 2;
@@ -318,14 +336,12 @@ int zo_ntt(const uint64_t* in, uint64_t* out, int64_t n, int invert, const uint6
     fpow_u64(step, g_m, 1ull << gs, &FR);
     power_table(g_hi, step, 1ll << (log_n - gs));
   }
-  if (coset && !invert) {
-    for (int64_t i = 0; i < n; ++i) {
-      int64_t r = 0;
-      for (int b = 0; b < log_n; ++b) r |= ((i >> b) & 1) << (log_n - 1 - b);
-      uint64_t g[4];
-      fmul(g, g_lo + 4 * (i & ((1ll << gs) - 1)), g_hi + 4 * (i >> gs), &FR);
-      fmul(out + 4 * r, out + 4 * r, g, &FR);
-    }
+  /* bit-reversed copy (zkgpu/ntt.py:132-141), with the forward coset scaling
+     x_j g^j (zkgpu/domain.py:33-39) applied on the way */
+  {
+    const int fwd_coset = coset && !invert;
+    bitrev_ctx c = {in, out, log_n, fwd_coset ? g_lo : NULL, fwd_coset ? g_hi : NULL, gs};
+    parallel_for(n, threads, bitrev_range, &c);
   }
   /* omega_n = w28^(2^28 / n), inverted for the inverse transform */
   uint64_t w[4];
