@@ -161,6 +161,35 @@ int zkb_ntt_cross_step(const zkb_field* f, const uint64_t* in, uint64_t* out, in
 int zkb_quotient_pointwise(const uint64_t* a, const uint64_t* b, const uint64_t* c,
                            const uint64_t* z, uint64_t* out, int64_t n, void* stream);
 
+/* ---- fields of one 64-bit word (moduli below 2^63) ------------------------ */
+
+/* Replace gpu_batch_mul / gpu_batch_add (zkgpu/field_gpu.py:147-196):
+ * out[i] = (a[i] OP b[i]) mod `mod`, for 2 <= mod < 2^63 (ZKB_EINVAL
+ * otherwise). Inputs are any int64 values, reduced into [0, mod) first (so
+ * negative ones land in the field); outputs lie in [0, mod). Device arrays of
+ * n int64; out may alias a or b. */
+int zkb_u64_mul(const int64_t* a, const int64_t* b, int64_t* out, int64_t n, int64_t mod, void* stream);
+int zkb_u64_add(const int64_t* a, const int64_t* b, int64_t* out, int64_t n, int64_t mod, void* stream);
+
+/* Replaces gpu_batch_pow (zkgpu/field_gpu.py:199-230) for a non-negative
+ * exponent: out[i] = bases[i]^e mod `mod`, e given as `words` little-endian
+ * 64-bit words in DEVICE memory (any size; words = 0 is e = 0). */
+int zkb_u64_pow(const int64_t* bases, int64_t* out, int64_t n, const uint64_t* exp_words, int words,
+                int64_t mod, void* stream);
+
+/* Device workspace (bytes) zkb_ntt64 needs for n words. */
+size_t zkb_ntt64_workspace_bytes(int64_t n);
+
+/* Replaces ntt_gpu (zkgpu/ntt_gpu.py:86-155): the natural-order NTT (or, with
+ * invert, its inverse scaled by n^-1) of n int64 values over an odd prime
+ * mod < 2^63, with omega the primitive n-th root of unity the caller derives
+ * (g^((mod-1)/n) for the smallest non-residue g, as zkgpu/ntt.py:98-124).
+ * Inputs are reduced into [0, mod) first; n a power of 2 up to 2^30; in and
+ * out must not overlap (ZKB_EINVAL). The workspace holds the stage twiddle
+ * table (16 KiB for any n). */
+int zkb_ntt64(const int64_t* in, int64_t* out, int64_t n, int64_t mod, int64_t omega, int invert,
+              void* workspace, size_t workspace_bytes, void* stream);
+
 /* ---- BN254 G1 ------------------------------------------------------------- */
 
 /* Replace the zk_g1_add / zk_g1_add_affine / zk_g1_double launches
@@ -269,8 +298,12 @@ int zkb_msm_batch(const zkb_msm_job* jobs, int count, void* workspace, size_t wo
  * does), "ntt.cta_log_elems" (log2 of the rows staged per NTT block, 9..12;
  * default 0 = 12 for large transforms, 10 when fewer than four 4096-row
  * blocks per SM), "ntt.threads" (threads per NTT block, 64..512; default 0 =
- * 512 for 4096-row blocks, else 256). ZKB_EINVAL for an unknown name or a
- * value out of range. Process-wide, not per stream. */
+ * 512 for 4096-row blocks, else 256); the int64 NTT's tile shapes
+ * "ntt64.first_col_log" (input words per row of a first-pass tile, log2, 0..6;
+ * -1 = by size), "ntt64.first_max_k" (first-pass stages, 4..10; 0 = by size),
+ * "ntt64.col_log" (words per row of a later-pass tile, log2, 1..6; 0 = by size),
+ * "ntt64.max_k" (most stages of a later pass, 2..10; 0 = by size). ZKB_EINVAL
+ * for an unknown name or a value out of range. Process-wide, not per stream. */
 int zkb_tune_set(const char* key, int value);
 int zkb_tune_get(const char* key, int* value);
 

@@ -140,6 +140,47 @@ def ntt(a: list[int], mod: int = R, invert: bool = False) -> list[int]:
     return a
 
 
+def ntt_np(a, mod: int, invert: bool = False):
+    """
+    The same transform on a NumPy int64 array, one vectorised stage at a time,
+    as the reference's ntt_gpu (zkgpu/ntt_gpu.py:128-153) runs it; for moduli
+    below 2^32, where every product fits uint64. Returns an int64 array.
+    """
+    import numpy as np
+
+    if mod >= 2**32:
+        raise ValueError("ntt_np needs mod < 2^32")
+    n = len(a)
+    omega = get_ntt_root(n, mod)
+    if invert:
+        omega = pow(omega, mod - 2, mod)
+    x = np.mod(np.asarray(a, dtype=np.int64), mod).astype(np.uint64)
+    if n == 1:
+        return x.astype(np.int64)
+    bits = n.bit_length() - 1
+    idx = np.arange(n, dtype=np.int64)
+    rev = np.zeros(n, dtype=np.int64)
+    for b in range(bits):
+        rev |= ((idx >> b) & 1) << (bits - 1 - b)
+    x = x[rev]
+    table = np.ones(n // 2, dtype=np.uint64)  # omega^j, j < n/2
+    for j in range(1, n // 2):
+        table[j] = table[j - 1] * np.uint64(omega) % np.uint64(mod)
+    m = np.uint64(mod)
+    length = 2
+    while length <= n:
+        half = length >> 1
+        groups = x.reshape(-1, length)
+        upper, lower = groups[:, :half].copy(), groups[:, half:]
+        v = lower * table[:: n // length] % m
+        groups[:, :half] = (upper + v) % m
+        groups[:, half:] = (upper + m - v) % m
+        length <<= 1
+    if invert:
+        x = x * np.uint64(pow(n, mod - 2, mod)) % m
+    return x.astype(np.int64)
+
+
 def scale_by_powers(values: list[int], g: int, mod: int) -> list[int]:
     """zkgpu/domain.py:33-39"""
     out, power = [], 1

@@ -18,6 +18,10 @@ Contents
   ntt.json    NTT / inverse / coset transforms, sizes 1..4096 in full, 2^16 and 2^20 by hash
   curve.json  exact Jacobian results of add / add_affine / double
   msm.json    Pippenger MSM results (small explicit cases; 2^12, 2^14, 2^16 by seed)
+  field64.json  int64-field mul/add/pow (zkgpu/field_gpu.py's CPU path) and NTTs over
+                moduli below 2^63, the moduli of the reference's own tests
+
+`--only field64.json` (or any other name) rewrites that file alone.
 """
 
 from __future__ import annotations
@@ -59,8 +63,12 @@ def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[1])
     ap.add_argument("--reference", default="/root/reference", help="reference checkout")
     ap.add_argument("--quick", action="store_true", help="skip the 2^16 MSM and 2^20 NTT")
+    ap.add_argument("--only", help="write this fixture file alone (field64.json)")
     args = ap.parse_args()
     sys.path.insert(0, str(Path(args.reference) / "src"))
+    if args.only == "field64.json":
+        field64_fixtures()
+        return
 
     from zkgpu import field256_gpu as ref_f256  # the reference's package
     from zkgpu.curve import (
@@ -269,6 +277,68 @@ def main() -> None:
                        "expected": pt(res)})
         print(f"msm {kind} 2^{n.bit_length() - 1}: {time.time() - t0:.1f}s", file=sys.stderr)
     dump("msm.json", {"cases": cases, "seeded": seeded})
+    field64_fixtures()
+
+
+def i64_digest(values: list[int]) -> str:
+    """SHA-256 of int64 values as little-endian 8-byte words (the GPU's output bytes)."""
+    return hashlib.sha256(b"".join(v.to_bytes(8, "little", signed=True) for v in values)).hexdigest()
+
+
+def field64_fixtures() -> None:
+    """
+    field64.json from the reference's int64 path: zkgpu/field_gpu.py with its
+    GPU flag off (its NumPy / Python-int fallback) and zkgpu/ntt.py's NTT, on
+    the moduli of the reference's tests/test_field_gpu.py:19-25 and
+    tests/test_ntt.py:14-35.
+    """
+    import warnings
+
+    import numpy as np
+    from zkgpu import field_gpu as ref_f64  # the reference's package
+    from zkgpu.ntt import ntt
+
+    warnings.simplefilter("ignore")
+    ref_f64._gpu_available = False
+    field_moduli = [7, 998_244_353, 3_037_000_500, 3_037_000_501, 2**61 - 1, 2**63 - 25]
+    primes = {7, 998_244_353, 2**61 - 1, 2**63 - 25}
+    ops = {}
+    for mod in field_moduli:
+        rng = random.Random(mod)
+        # operands over all of int64: negative and unreduced values included
+        a = [rng.randrange(-(2**63), 2**63) for _ in range(64)] + [mod - 1, 0, 2**63 - 1, -(2**63)]
+        b = [rng.randrange(-(2**63), 2**63) for _ in range(64)] + [mod - 1, mod - 1, -(2**63), 2**63 - 1]
+        A, B = np.array(a, dtype=np.int64), np.array(b, dtype=np.int64)
+        entry = {
+            "a": a,
+            "b": b,
+            "mul": ref_f64.gpu_batch_mul(A, B, mod).tolist(),
+            "add": ref_f64.gpu_batch_add(A, B, mod).tolist(),
+            "pow": {str(e): ref_f64.gpu_batch_pow(B, e, mod).tolist() for e in (0, 1, 2, 65537, 2**70 + 3)},
+        }
+        if mod in primes:
+            inv = [v if v % mod else 1 for v in a]  # zero has no inverse
+            entry["inv_bases"] = inv
+            entry["pow"]["-3"] = ref_f64.gpu_batch_pow(np.array(inv, dtype=np.int64), -3, mod).tolist()
+        ops[str(mod)] = entry
+    ntt_moduli = [998_244_353, 12_289, 2_147_483_641 * 2**32 + 1]
+    transforms = {}
+    for mod in ntt_moduli:
+        per = {}
+        for n in (1, 2, 8, 256, 4096):
+            rng = random.Random(n)  # the reference test's draw (tests/test_ntt.py:226-229)
+            a = [rng.randrange(mod) for _ in range(n)]
+            fwd, inv = ntt(a, mod), ntt(a, mod, invert=True)
+            if n <= 256:
+                per[str(n)] = {"fwd": fwd, "inv": inv}
+            else:
+                per[str(n)] = {"fwd_sha256": i64_digest(fwd), "inv_sha256": i64_digest(inv),
+                               "fwd_samples": {str(i): fwd[i] for i in (0, 1, n // 2, n - 1)}}
+        edge = [mod + 5, 2 * mod + 1 if 2 * mod + 1 <= 2**63 - 1 else -1, 2**63 - 1, -(2**63)] + [0] * 4
+        per["unreduced"] = {"input": edge, "fwd": ntt(edge, mod), "inv": ntt(edge, mod, invert=True)}
+        transforms[str(mod)] = per
+    (HERE / "field64.json").write_text(json.dumps({"ops": ops, "ntt": transforms}, sort_keys=True) + "\n")
+    print("wrote field64.json", file=sys.stderr)
 
 
 if __name__ == "__main__":

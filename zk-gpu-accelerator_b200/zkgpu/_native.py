@@ -104,6 +104,11 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
         [_fp, _u64p, _u64p, _i64, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64),
          _u64p, _vp],
     ),
+    "zkb_u64_mul": (ctypes.c_int, [_u64p, _u64p, _u64p, _i64, _i64, _vp]),
+    "zkb_u64_add": (ctypes.c_int, [_u64p, _u64p, _u64p, _i64, _i64, _vp]),
+    "zkb_u64_pow": (ctypes.c_int, [_u64p, _u64p, _i64, _u64p, ctypes.c_int, _i64, _vp]),
+    "zkb_ntt64_workspace_bytes": (ctypes.c_size_t, [_i64]),
+    "zkb_ntt64": (ctypes.c_int, [_u64p, _u64p, _i64, _i64, _i64, ctypes.c_int, _vp, ctypes.c_size_t, _vp]),
     "zkb_g1_add": (ctypes.c_int, [_u64p, _i64, _u64p, _i64, _u64p, _i64, _vp]),
     "zkb_g1_add_affine": (ctypes.c_int, [_u64p, _i64, _u64p, _i64, _u64p, _i64, _vp]),
     "zkb_g1_double": (ctypes.c_int, [_u64p, _u64p, _i64, _vp]),
