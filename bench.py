@@ -80,7 +80,9 @@ def _peaks() -> dict:
 # ------------------------------------------------------------------
 
 IMAD_PER_MULMOD = 264  # 2 x 64 32-bit multiply-adds (lo and hi) for a*b and m*p, plus 8 for the m's
-MULMOD_PER_MADD = 10   # XYZZ mixed addition: 8 multiplications + 2 squarings
+IMAD_PER_SQR = 208     # 2 x (36 + 64) for a*a (each cross product once) and m*p, plus 8 for the m's
+# XYZZ mixed addition: 8 multiplications + 2 squarings
+IMAD_PER_MADD = 8 * IMAD_PER_MULMOD + 2 * IMAD_PER_SQR
 
 
 # GLV split constants (csrc/msm.cu): k = k1 + k2 lambda, c1 = floor(k g1 / 2^256), ...
@@ -399,7 +401,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     def acc_roof(madds: int, prof: dict, kernel: str, traffic) -> dict:
         count, total = prof.get("msm_acc_points", (1, float("nan")))
         ms = total / max(count, 1)
-        imad = madds * MULMOD_PER_MADD * IMAD_PER_MULMOD
+        imad = madds * IMAD_PER_MADD
         achieved = imad / (ms * 1e-3) / 1e12
         acc_bytes = madds * (64 + 8) + 2 * (-(-madds // 64)) * 132  # point gathers + sorted pairs + slots
         return {
@@ -407,7 +409,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
             "unit": "TIMAD/s", "frac": round(achieved / imad_peak_t, 4), "traffic": traffic,
             "peak_source": f"nominal issue rate: {sm_count} SMs x 64 IMAD/clk x {mhz:.0f} MHz (median SM clock "
                            "sampled in the timed region)",
-            "work_per_launch": f"{madds} mixed additions x {MULMOD_PER_MADD} mulmod x {IMAD_PER_MULMOD} IMAD",
+            "work_per_launch": f"{madds} mixed additions x (8 x {IMAD_PER_MULMOD} + 2 x {IMAD_PER_SQR}) IMAD",
             "launch_ms": round(ms, 4), "launches": count,
             "hbm": {"achieved": round(acc_bytes / (ms * 1e-3) / 1e9, 1), "peak": hbm_peak, "unit": "GB/s",
                     "frac": round(acc_bytes / (ms * 1e-3) / 1e9 / hbm_peak, 4) if hbm_peak else None,

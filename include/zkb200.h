@@ -70,7 +70,9 @@ int zkb_field_init(zkb_field* f, const uint64_t modulus[4]);
 /* Replaces the zk256_mul / zk256_add / zk256_sub launches with their
  * single-row broadcast (zkgpu/field256_gpu.py:172-191, :466-473):
  * out[i] = a[i * a_step] OP b[i * b_step] for i < n, where a_step and b_step
- * are 1, or 0 to broadcast one row. n = 0 is a no-op. out may alias a or b. */
+ * are 1, or 0 to broadcast one row. n = 0 is a no-op. out may alias a or b.
+ * zkb_field_mul with a == b and equal steps squares (36 word products in
+ * place of 64; the same rows). */
 int zkb_field_mul(const zkb_field* f, const uint64_t* a, int64_t a_step, const uint64_t* b,
                   int64_t b_step, uint64_t* out, int64_t n, void* stream);
 int zkb_field_add(const zkb_field* f, const uint64_t* a, int64_t a_step, const uint64_t* b,

@@ -92,6 +92,21 @@ def test_ops_match_python(field, op):
     assert got == [fn(x, y) % p for x, y in zip(a, b, strict=True)]
 
 
+@pytest.mark.parametrize("field", FIELDS)
+def test_squaring_matches_python(field):
+    """mul(x, x) on the same rows takes the squaring path (separated operand scanning): exact
+    against Python integers on random values and the carry-heavy edges, broadcast row included."""
+    F = field
+    p = F.modulus
+    rng = random.Random(p % 997)
+    values = [0, 1, 2, p - 1, p - 2, (p - 1) // 2, (p + 1) // 2] + [rng.randrange(p) for _ in range(4000)]
+    values += [min(p - 1, (1 << k) - 1) for k in range(1, p.bit_length() + 1)]
+    rows = F.from_ints(values)
+    assert F.to_ints(F.mul(rows, rows)) == [v * v % p for v in values]
+    one = F.from_ints([p - 1])
+    assert F.to_ints(F.mul(one, one)) == [1]
+
+
 def test_operations_compose():
     F, p = BN254_FQ, P
     a, b = operands(p, 4)

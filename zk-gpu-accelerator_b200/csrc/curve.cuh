@@ -248,11 +248,15 @@ struct InlineMul {
   __device__ __forceinline__ static void mul(uint32_t r[8], const uint32_t a[8], const uint32_t b[8]) {
     fe_mul(r, a, b, G1F{});
   }
+  __device__ __forceinline__ static void sqr(uint32_t r[8], const uint32_t a[8]) { fe_sqr(r, a, G1F{}); }
 };
 
 struct CallMul {
   __device__ __forceinline__ static void mul(uint32_t r[8], const uint32_t a[8], const uint32_t b[8]) {
     fe_mul_shared(r, a, b, G1F{});
+  }
+  __device__ __forceinline__ static void sqr(uint32_t r[8], const uint32_t a[8]) {
+    fe_sqr_shared(r, a, G1F{});
   }
 };
 
@@ -263,13 +267,13 @@ __device__ __forceinline__ void xyzz_mdbl(Xyzz& r, const Aff& q) {
   G1F f;
   uint32_t u[8], v[8], w[8], s[8], m[8], t[8];
   fe_dbl(u, q.y, f);
-  M::mul(v, u, u);
+  M::sqr(v, u);
   M::mul(w, u, v);
   M::mul(s, q.x, v);
-  M::mul(m, q.x, q.x);
+  M::sqr(m, q.x);
   fe_dbl(t, m, f);
   fe_add(m, m, t, f);
-  M::mul(r.x, m, m);
+  M::sqr(r.x, m);
   fe_dbl(t, s, f);
   fe_sub(r.x, r.x, t, f);
   fe_sub(t, s, r.x, f);
@@ -291,14 +295,14 @@ __device__ __forceinline__ void xyzz_dbl(Xyzz& r, const Xyzz& p) {
   }
   uint32_t u[8], v[8], w[8], s[8], m[8], t[8];
   fe_dbl(u, p.y, f);
-  M::mul(v, u, u);
+  M::sqr(v, u);
   M::mul(w, u, v);
   M::mul(s, p.x, v);
-  M::mul(m, p.x, p.x);
+  M::sqr(m, p.x);
   fe_dbl(t, m, f);
   fe_add(m, m, t, f);
   uint32_t x3[8], y3[8];
-  M::mul(x3, m, m);
+  M::sqr(x3, m);
   fe_dbl(t, s, f);
   fe_sub(x3, x3, t, f);
   fe_sub(t, s, x3, f);
@@ -336,12 +340,12 @@ __device__ __forceinline__ void xyzz_add_affine(Xyzz& acc, const Aff& q) {
     return;
   }
   uint32_t ppp[8], qq[8];
-  M::mul(t, pp, pp);           // PP
+  M::sqr(t, pp);           // PP
   M::mul(ppp, pp, t);      // PPP
   M::mul(qq, acc.x, t);    // Q
   M::mul(acc.zz, acc.zz, t);
   M::mul(acc.zzz, acc.zzz, ppp);
-  M::mul(t, r, r);
+  M::sqr(t, r);
   fe_sub(t, t, ppp, f);
   fe_sub(t, t, qq, f);
   fe_sub(t, t, qq, f);        // X3
@@ -383,14 +387,14 @@ __device__ __forceinline__ void xyzz_add(Xyzz& r, const Xyzz& p, const Xyzz& q) 
     return;
   }
   uint32_t ppp[8], qq[8], zz[8], zzz[8];
-  M::mul(t, pp, pp);           // PP
+  M::sqr(t, pp);           // PP
   M::mul(ppp, pp, t);      // PPP
   M::mul(qq, u1, t);       // Q
   M::mul(zz, p.zz, q.zz);
   M::mul(zz, zz, t);
   M::mul(zzz, p.zzz, q.zzz);
   M::mul(zzz, zzz, ppp);
-  M::mul(t, rr, rr);
+  M::sqr(t, rr);
   fe_sub(t, t, ppp, f);
   fe_sub(t, t, qq, f);
   fe_sub(t, t, qq, f);        // X3

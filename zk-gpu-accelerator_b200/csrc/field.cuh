@@ -281,9 +281,67 @@ __device__ __forceinline__ void fe_mul(uint32_t r[8], const uint32_t a[8], const
   fe_copy(r, t);
 }
 
+// r = a^2 * 2^-256 mod p, canonical; r may alias a.
+//
+// SOS (separated operand scanning): the 512-bit square first, each
+// off-diagonal product a_i a_j (i < j) computed once and the sum doubled,
+// then the diagonal a_i^2: 36 word products instead of 64. Then eight
+// Montgomery rows t = t + m p 2^(32 i), m = t_i (-p^-1) mod 2^32, as in fe_mul
+// (64 products). With a < p < 2^255 every partial sum stays below 2^512, so
+// 16 words hold it, and the result (t / 2^256 < 2p) needs one conditional
+// subtraction. A row's carry out of word i + 8 (0 or 1) is added one word
+// higher by the next row.
 template <class F>
 __device__ __forceinline__ void fe_sqr(uint32_t r[8], const uint32_t a[8], const F& f) {
-  fe_mul(r, a, a, f);
+  uint32_t x[8], t[16];
+  fe_copy(x, a);
+#pragma unroll
+  for (int k = 0; k < 16; ++k) t[k] = 0;
+#pragma unroll
+  for (int i = 0; i < 7; ++i) {
+    uint64_t c = 0;
+#pragma unroll
+    for (int j = i + 1; j < 8; ++j) {
+      const uint64_t q = (uint64_t)x[i] * x[j] + t[i + j] + c;
+      t[i + j] = (uint32_t)q;
+      c = q >> 32;
+    }
+    t[i + 8] = (uint32_t)c;  // no earlier row reached word i + 8
+  }
+  // double the off-diagonal sum (words 1..14 -> 1..15)
+  t[15] = t[14] >> 31;
+#pragma unroll
+  for (int k = 14; k >= 1; --k) t[k] = __funnelshift_l(t[k - 1], t[k], 1);
+  uint64_t c = 0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    uint64_t q = (uint64_t)x[i] * x[i] + t[2 * i] + c;
+    t[2 * i] = (uint32_t)q;
+    q = (uint64_t)t[2 * i + 1] + (q >> 32);
+    t[2 * i + 1] = (uint32_t)q;
+    c = q >> 32;
+  }
+  uint32_t hc = 0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const uint32_t m = t[i] * f.ninv();
+    uint64_t q = (uint64_t)m * f.p(0) + t[i];
+    c = q >> 32;
+#pragma unroll
+    for (int j = 1; j < 8; ++j) {
+      q = (uint64_t)m * f.p(j) + t[i + j] + c;
+      t[i + j] = (uint32_t)q;
+      c = q >> 32;
+    }
+    q = (uint64_t)t[i + 8] + c + hc;
+    t[i + 8] = (uint32_t)q;
+    hc = (uint32_t)(q >> 32);
+  }
+  uint32_t out[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) out[j] = t[8 + j];
+  fe_reduce_once(out, f);
+  fe_copy(r, out);
 }
 
 // ---- one shared copy of the product ----------------------------------------
@@ -303,6 +361,28 @@ static __device__ __noinline__ Fe8 fe_mul_outlined(const Fe8 a, const Fe8 b) {
   Fe8 r;
   fe_mul(r.w, a.w, b.w, F{});
   return r;
+}
+
+template <class F>
+static __device__ __noinline__ Fe8 fe_sqr_outlined(const Fe8 a) {
+  Fe8 r;
+  fe_sqr(r.w, a.w, F{});
+  return r;
+}
+
+// the squaring's shared copy, as fe_mul_shared
+template <class F>
+__device__ __forceinline__ void fe_sqr_shared(uint32_t r[8], const uint32_t a[8], const F&) {
+  Fe8 x;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) x.w[j] = a[j];
+  const Fe8 z = fe_sqr_outlined<F>(x);
+#pragma unroll
+  for (int j = 0; j < 8; ++j) r[j] = z.w[j];
+}
+
+__device__ __forceinline__ void fe_sqr_shared(uint32_t r[8], const uint32_t a[8], const FieldRT& f) {
+  fe_sqr(r, a, f);
 }
 
 template <class F>

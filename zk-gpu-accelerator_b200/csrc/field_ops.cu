@@ -20,7 +20,9 @@ __global__ void __launch_bounds__(256) k_field_binary(F f, const uint64_t* a, in
     uint32_t x[8], y[8], r[8];
     fe_load(x, a + 4 * i * a_step);
     fe_load(y, b + 4 * i * b_step);
-    if (OP == OP_MUL) {
+    if (OP == OP_MUL && a == b && a_step == b_step) {
+      fe_sqr(r, x, f);  // the same rows on both sides: the squaring's 36-product form
+    } else if (OP == OP_MUL) {
       fe_mul(r, x, y, f);
     } else if (OP == OP_ADD) {
       fe_add(r, x, y, f);
