@@ -304,8 +304,12 @@ int zkb_msm_batch(const zkb_msm_job* jobs, int count, void* workspace, size_t wo
  * "ntt64.first_col_log" (input words per row of a first-pass tile, log2, 0..6;
  * -1 = by size), "ntt64.first_max_k" (first-pass stages, 4..10; 0 = by size),
  * "ntt64.col_log" (words per row of a later-pass tile, log2, 1..6; 0 = by size),
- * "ntt64.max_k" (most stages of a later pass, 2..10; 0 = by size). ZKB_EINVAL
- * for an unknown name or a value out of range. Process-wide, not per stream. */
+ * "ntt64.max_k" (most stages of a later pass, 2..10; 0 = by size);
+ * "ntt.full_table_mb" (MiB the library may hold in expanded NTT tables: per
+ * transform size the n twiddles w_n^i, per coset transform its n scale
+ * factors, each saving one product per row; default 4096, 0 = none).
+ * ZKB_EINVAL for an unknown name or a value out of range. Process-wide, not
+ * per stream. */
 int zkb_tune_set(const char* key, int value);
 int zkb_tune_get(const char* key, int* value);
 

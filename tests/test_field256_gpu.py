@@ -221,6 +221,8 @@ def test_ntt_matches_c_oracle_between_fixture_sizes(log_n):
         {"ntt.max_log_radix": 9, "ntt.cta_log_elems": 9, "ntt.threads": 64},
         {"ntt.cta_log_elems": 12, "ntt.threads": 128},
         {"ntt.cta_log_elems": 10, "ntt.threads": 512},
+        {"ntt.full_table_mb": 0},  # two-level twiddle and coset tables only
+        {"ntt.max_log_radix": 8, "ntt.full_table_mb": 1},  # expanded tables for the small sizes only
     ],
 )
 def test_ntt_pass_plans_give_the_same_rows(knobs):
@@ -253,6 +255,7 @@ def test_ntt_pass_plans_give_the_same_rows(knobs):
         _native.tune_set("ntt.max_log_radix", 12)
         _native.tune_set("ntt.cta_log_elems", 0)
         _native.tune_set("ntt.threads", 0)
+        _native.tune_set("ntt.full_table_mb", 4096)
 
 
 def test_ntt_2_24_config_size():

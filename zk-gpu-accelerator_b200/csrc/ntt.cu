@@ -58,6 +58,8 @@ struct ScaleTables {
   uint64_t* g_lo = nullptr;
   uint64_t* g_hi = nullptr;
   uint64_t* scale = nullptr;  // one element: n^-1 (Montgomery)
+  uint64_t* g_full = nullptr; // optional: the n products g_lo g_hi themselves (byte budget)
+  size_t full_bytes = 0;
   int gs = 0;
 };
 
@@ -108,6 +110,23 @@ __global__ void k_pow_table(F f, const uint64_t* base, const uint64_t* pre, uint
       fe_mul(r, r, p, f);
     }
     fe_store(out + 4 * i, r);
+  }
+}
+
+// out[i] = lo[(i << shift) & mask] * hi[(i << shift) >> s] for i < count: a two-level
+// table expanded into one row per index (one product each).
+template <class F>
+__global__ void k_expand_table(F f, const uint64_t* lo, const uint64_t* hi, int s, int shift,
+                               uint64_t* out, int64_t count) {
+  const uint64_t mask = (1ull << s) - 1;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride) {
+    const uint64_t e = (uint64_t)i << shift;
+    uint32_t a[8], b[8];
+    fe_load_nc(a, lo + 4 * (e & mask));
+    fe_load_nc(b, hi + 4 * (e >> s));
+    fe_mul(a, a, b, f);
+    fe_store(out + 4 * i, a);
   }
 }
 
@@ -180,6 +199,22 @@ static constexpr size_t kMaxRootEntries = 16;  // like the reference's lru_cache
 // At least the 64 transforms of one batch, whose tables must all stay alive
 // until its launch (an entry used in the batch is never the least recent).
 static constexpr size_t kMaxScaleEntries = 96;
+
+// Expanded tables of single transforms (never of batches, whose tables must stay
+// alive until their one launch): per (root, size) the n powers w_n^i, and in a
+// scale entry the n coset / inverse factors. Together they stay within the byte
+// budget "ntt.full_table_mb"; a table that does not fit is not built and the
+// pass falls back to the two-level tables (one more product per row).
+struct FullEntry {
+  TableKey key;
+  int log_n;
+  uint64_t* w;
+  size_t bytes;
+};
+static std::list<FullEntry> g_fulls;  // most recently used first
+static size_t g_full_bytes = 0;
+static constexpr size_t kMaxFullEntries = 16;
+static constexpr int kMinFullLog = 10;  // below, transforms are one pass with no boundary twiddle
 
 template <class F>
 static int build_roots(const F& f, const TableKey& key, RootTables& t, void** mem,
@@ -262,6 +297,11 @@ struct NttPass {
   const uint64_t* g_lo; // coset tables (null without a coset)
   const uint64_t* g_hi;
   int gs;
+  // optional expanded tables (null: use the two-level ones): t_full[i] = w_n^i for
+  // i < n, indexed by e >> full_shift; g_full[j] = the coset / inverse scale of row j
+  const uint64_t* t_full;
+  int full_shift;
+  const uint64_t* g_full;
   const uint64_t* scale;  // n^-1 for an inverse transform without coset tables
 };
 
@@ -355,11 +395,16 @@ __device__ __forceinline__ void ntt_tile(const F& f, const NttPass& a, int64_t b
       fe_load_nc(x, a.in + 4 * pos);
     }
     if (a.first && a.g_lo && !a.inverse) {
-      const uint64_t m = (1ull << a.gs) - 1;
-      uint32_t lo[8], hi[8];
-      fe_load_nc(lo, a.g_lo + 4 * ((uint64_t)pos & m));
-      fe_load_nc(hi, a.g_hi + 4 * ((uint64_t)pos >> a.gs));
-      ntt_mul<kShared>(lo, lo, hi, f);
+      uint32_t lo[8];
+      if (a.g_full) {
+        fe_load_nc(lo, a.g_full + 4 * pos);
+      } else {
+        const uint64_t m = (1ull << a.gs) - 1;
+        uint32_t hi[8];
+        fe_load_nc(lo, a.g_lo + 4 * ((uint64_t)pos & m));
+        fe_load_nc(hi, a.g_hi + 4 * ((uint64_t)pos >> a.gs));
+        ntt_mul<kShared>(lo, lo, hi, f);
+      }
       ntt_mul<kShared>(x, x, lo, f);
     }
     fe_store(sm + sm_index(c, jr, lr), x);
@@ -449,7 +494,11 @@ __device__ __forceinline__ void ntt_tile(const F& f, const NttPass& a, int64_t b
       if (a.inverse && e) e = (1ull << a.log_N) - e;
       if (e) {
         uint32_t tw[8];
-        root_power<kShared>(tw, a, e, f);
+        if (a.t_full) {
+          fe_load_nc(tw, a.t_full + 4 * (e >> a.full_shift));
+        } else {
+          root_power<kShared>(tw, a, e, f);
+        }
         ntt_mul<kShared>(x, x, tw, f);
       }
       const int64_t pos = o * B + (int64_t)k * S + jp;
@@ -460,7 +509,9 @@ __device__ __forceinline__ void ntt_tile(const F& f, const NttPass& a, int64_t b
                              ((int64_t)k << (a.log_n - lr));
       if (a.inverse) {
         uint32_t sc[8];
-        if (a.g_lo) {
+        if (a.g_full) {
+          fe_load_nc(sc, a.g_full + 4 * outidx);
+        } else if (a.g_lo) {
           const uint64_t m = (1ull << a.gs) - 1;
           uint32_t lo[8], hi[8];
           fe_load_nc(lo, a.g_lo + 4 * ((uint64_t)outidx & m));
@@ -649,12 +700,90 @@ static int lookup_tables(const F& f, const TableKey& key, int64_t n, int log_n, 
     if (g_scales.size() > kMaxScaleEntries) {
       cudaDeviceSynchronize();
       cudaFree(g_scales.back().mem);
+      if (g_scales.back().t.g_full) {
+        cudaFree(g_scales.back().t.g_full);
+        g_full_bytes -= g_scales.back().t.full_bytes;
+      }
       g_scales.pop_back();
     }
   } else {
     g_scales.splice(g_scales.begin(), g_scales, jt);
   }
   st = g_scales.front().t;
+  return ZKB_OK;
+}
+
+// The expanded tables of one single transform of n = 2^log_n rows: the root
+// powers w_n^i (t_full, shared by both directions) and, for a coset transform,
+// its scale factors inside the scale entry (st->g_full). Either is left null
+// when it does not fit the byte budget.
+template <class F>
+static int lookup_full(const F& f, const TableKey& key, const RootTables& rt, int64_t n, int log_n,
+                       ScaleTables* st, const uint64_t** t_full, cudaStream_t s) {
+  *t_full = nullptr;
+  const size_t budget = (size_t)tune_get("ntt.full_table_mb") << 20;
+  if (log_n < kMinFullLog || budget == 0) {
+    st->g_full = nullptr;  // a budget of 0 means the two-level tables, cached expansions or not
+    return ZKB_OK;
+  }
+  const size_t bytes = (size_t)n * 32;
+  std::lock_guard<std::mutex> lock(g_ntt_mutex);
+  auto it = g_fulls.begin();
+  for (; it != g_fulls.end(); ++it)
+    if (it->key == key && it->log_n == log_n) break;
+  if (it != g_fulls.end()) {
+    g_fulls.splice(g_fulls.begin(), g_fulls, it);
+    *t_full = g_fulls.front().w;
+  } else {
+    // room among the expanded root tables, least recently used first
+    while (g_full_bytes + bytes > budget && !g_fulls.empty()) {
+      cudaDeviceSynchronize();  // kernels queued on any stream may still read it
+      cudaFree(g_fulls.back().w);
+      g_full_bytes -= g_fulls.back().bytes;
+      g_fulls.pop_back();
+    }
+    if (g_full_bytes + bytes <= budget) {
+      FullEntry e{key, log_n, nullptr, bytes};
+      ZKB_TRY(check_cuda(cudaMalloc(&e.w, bytes), "NTT expanded root table allocation"));
+      k_expand_table<<<grid_for(n, 128), 128, 0, s>>>(f, rt.t_lo, rt.t_hi, rt.s, rt.log_N - log_n, e.w, n);
+      int rc = check_launch("NTT expanded root table");
+      if (rc == ZKB_OK) rc = check_cuda(cudaStreamSynchronize(s), "NTT expanded root table build");
+      if (rc != ZKB_OK) {
+        cudaFree(e.w);
+        return rc;
+      }
+      g_fulls.push_front(e);
+      g_full_bytes += bytes;
+      if (g_fulls.size() > kMaxFullEntries) {
+        cudaDeviceSynchronize();
+        cudaFree(g_fulls.back().w);
+        g_full_bytes -= g_fulls.back().bytes;
+        g_fulls.pop_back();
+      }
+      *t_full = e.w;
+    }
+  }
+  if (st->g_lo && !st->g_full && g_full_bytes + bytes <= budget) {
+    for (ScaleEntry& e : g_scales) {
+      if (e.t.g_lo != st->g_lo) continue;
+      if (!e.t.g_full) {
+        uint64_t* g = nullptr;
+        ZKB_TRY(check_cuda(cudaMalloc(&g, bytes), "NTT expanded scale table allocation"));
+        k_expand_table<<<grid_for(n, 128), 128, 0, s>>>(f, e.t.g_lo, e.t.g_hi, e.t.gs, 0, g, n);
+        int rc = check_launch("NTT expanded scale table");
+        if (rc == ZKB_OK) rc = check_cuda(cudaStreamSynchronize(s), "NTT expanded scale table build");
+        if (rc != ZKB_OK) {
+          cudaFree(g);
+          return rc;
+        }
+        e.t.g_full = g;
+        e.t.full_bytes = bytes;
+        g_full_bytes += bytes;
+      }
+      st->g_full = e.t.g_full;
+      break;
+    }
+  }
   return ZKB_OK;
 }
 
@@ -729,6 +858,7 @@ static void plan_passes(int64_t n, int log_n, int invert, const RootTables& rt,
     a.g_hi = st.g_hi;
     a.gs = st.gs;
     a.scale = st.scale;
+    a.g_full = st.g_full;
     int lc = cta_log > a.lr ? cta_log - a.lr : 0;
     if (!a.last) {
       if (lc > a.ls) lc = a.ls;
@@ -767,6 +897,8 @@ static int run_ntt(const F& f, const zkb_field* field, const uint64_t* in, uint6
   RootTables rt;
   ScaleTables st;
   ZKB_TRY(lookup_tables(f, key, n, log_n, invert, coset, rt, st, s));
+  const uint64_t* t_full = nullptr;
+  ZKB_TRY(lookup_full(f, key, rt, n, log_n, &st, &t_full, s));
 
   const size_t need = workspace_bytes(n);
   if (need && (!workspace || ws_bytes < need)) {
@@ -780,6 +912,8 @@ static int run_ntt(const F& f, const zkb_field* field, const uint64_t* in, uint6
               0, passes);
   const int P = (int)passes.size();
   for (int q = 0; q < P; ++q) {
+    passes[q].a.t_full = t_full;
+    passes[q].a.full_shift = rt.log_N - log_n;
     const PassLaunch& L = passes[q];
     auto kern = tune_get("ntt.call_products") ? k_ntt_pass<F, true> : k_ntt_pass<F, false>;
     ZKB_TRY(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
