@@ -306,8 +306,9 @@ int zkb_msm_batch(const zkb_msm_job* jobs, int count, void* workspace, size_t wo
  * "ntt64.col_log" (words per row of a later-pass tile, log2, 1..6; 0 = by size),
  * "ntt64.max_k" (most stages of a later pass, 2..10; 0 = by size);
  * "ntt.full_table_mb" (MiB the library may hold in expanded NTT tables: per
- * transform size the n twiddles w_n^i, per coset transform its n scale
- * factors, each saving one product per row; default 4096, 0 = none).
+ * pass shape and direction the boundary twiddles of a non-last pass, per
+ * coset transform its n scale factors, each saving one product per row;
+ * default 4096, 0 = none).
  * ZKB_EINVAL for an unknown name or a value out of range. Process-wide, not
  * per stream. */
 int zkb_tune_set(const char* key, int value);

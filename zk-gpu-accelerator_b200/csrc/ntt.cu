@@ -201,13 +201,14 @@ static constexpr size_t kMaxRootEntries = 16;  // like the reference's lru_cache
 static constexpr size_t kMaxScaleEntries = 96;
 
 // Expanded tables of single transforms (never of batches, whose tables must stay
-// alive until their one launch): per (root, size) the n powers w_n^i, and in a
-// scale entry the n coset / inverse factors. Together they stay within the byte
-// budget "ntt.full_table_mb"; a table that does not fit is not built and the
-// pass falls back to the two-level tables (one more product per row).
+// alive until their one launch): per (root, pass shape, direction) the boundary
+// twiddles of a non-last pass laid out as its rows read them, and in a scale
+// entry the n coset / inverse factors. Together they stay within the byte budget
+// "ntt.full_table_mb"; a table that does not fit is not built and the pass falls
+// back to the two-level tables (one more product per row).
 struct FullEntry {
   TableKey key;
-  int log_n;
+  int lr, ls, inverse;
   uint64_t* w;
   size_t bytes;
 };
@@ -297,10 +298,10 @@ struct NttPass {
   const uint64_t* g_lo; // coset tables (null without a coset)
   const uint64_t* g_hi;
   int gs;
-  // optional expanded tables (null: use the two-level ones): t_full[i] = w_n^i for
-  // i < n, indexed by e >> full_shift; g_full[j] = the coset / inverse scale of row j
+  // optional expanded tables (null: use the two-level ones): t_full[(k << ls) + j] =
+  // the boundary twiddle of row k, column j of a non-last pass; g_full[j] = the
+  // coset / inverse scale of row j
   const uint64_t* t_full;
-  int full_shift;
   const uint64_t* g_full;
   const uint64_t* scale;  // n^-1 for an inverse transform without coset tables
 };
@@ -495,7 +496,7 @@ __device__ __forceinline__ void ntt_tile(const F& f, const NttPass& a, int64_t b
       if (e) {
         uint32_t tw[8];
         if (a.t_full) {
-          fe_load_nc(tw, a.t_full + 4 * (e >> a.full_shift));
+          fe_load_nc(tw, a.t_full + 4 * (((int64_t)k << a.ls) + jp));
         } else {
           root_power<kShared>(tw, a, e, f);
         }
@@ -713,24 +714,41 @@ static int lookup_tables(const F& f, const TableKey& key, int64_t n, int log_n, 
   return ZKB_OK;
 }
 
-// The expanded tables of one single transform of n = 2^log_n rows: the root
-// powers w_n^i (t_full, shared by both directions) and, for a coset transform,
-// its scale factors inside the scale entry (st->g_full). Either is left null
-// when it does not fit the byte budget.
+// The boundary twiddles of a non-last pass of 2^lr rows at stride 2^ls, as its
+// store reads them: out[(k << ls) + j] = w_B^(j k) (w_B^-(j k) inverse) for
+// k < 2^lr, j < 2^ls, B = 2^(lr + ls), from the two-level root tables, so that
+// neighbouring columns of a row read neighbouring entries.
 template <class F>
-static int lookup_full(const F& f, const TableKey& key, const RootTables& rt, int64_t n, int log_n,
-                       ScaleTables* st, const uint64_t** t_full, cudaStream_t s) {
+__global__ void k_expand_twiddles(F f, const uint64_t* lo, const uint64_t* hi, int s, int log_N, int lr,
+                                  int ls, int inverse, uint64_t* out) {
+  const uint64_t mask = (1ull << s) - 1;
+  const int64_t count = 1ll << (lr + ls);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride) {
+    const uint64_t k = (uint64_t)i >> ls, j = (uint64_t)i & ((1ull << ls) - 1);
+    uint64_t e = (j * k) << (log_N - (lr + ls));
+    if (inverse && e) e = (1ull << log_N) - e;
+    uint32_t a[8], b[8];
+    fe_load_nc(a, lo + 4 * (e & mask));
+    fe_load_nc(b, hi + 4 * (e >> s));
+    fe_mul(a, a, b, f);
+    fe_store(out + 4 * i, a);
+  }
+}
+
+// The expanded boundary twiddles of a non-last pass (null when they do not fit
+// the byte budget, or the budget is 0).
+template <class F>
+static int lookup_twiddles(const F& f, const TableKey& key, const RootTables& rt, int lr, int ls, int inverse,
+                           const uint64_t** t_full, cudaStream_t s) {
   *t_full = nullptr;
   const size_t budget = (size_t)tune_get("ntt.full_table_mb") << 20;
-  if (log_n < kMinFullLog || budget == 0) {
-    st->g_full = nullptr;  // a budget of 0 means the two-level tables, cached expansions or not
-    return ZKB_OK;
-  }
-  const size_t bytes = (size_t)n * 32;
+  if (lr + ls < kMinFullLog || budget == 0) return ZKB_OK;
+  const size_t bytes = (size_t)32 << (lr + ls);
   std::lock_guard<std::mutex> lock(g_ntt_mutex);
   auto it = g_fulls.begin();
   for (; it != g_fulls.end(); ++it)
-    if (it->key == key && it->log_n == log_n) break;
+    if (it->key == key && it->lr == lr && it->ls == ls && it->inverse == inverse) break;
   if (it != g_fulls.end()) {
     g_fulls.splice(g_fulls.begin(), g_fulls, it);
     *t_full = g_fulls.front().w;
@@ -743,11 +761,12 @@ static int lookup_full(const F& f, const TableKey& key, const RootTables& rt, in
       g_fulls.pop_back();
     }
     if (g_full_bytes + bytes <= budget) {
-      FullEntry e{key, log_n, nullptr, bytes};
-      ZKB_TRY(check_cuda(cudaMalloc(&e.w, bytes), "NTT expanded root table allocation"));
-      k_expand_table<<<grid_for(n, 128), 128, 0, s>>>(f, rt.t_lo, rt.t_hi, rt.s, rt.log_N - log_n, e.w, n);
-      int rc = check_launch("NTT expanded root table");
-      if (rc == ZKB_OK) rc = check_cuda(cudaStreamSynchronize(s), "NTT expanded root table build");
+      FullEntry e{key, lr, ls, inverse, nullptr, bytes};
+      ZKB_TRY(check_cuda(cudaMalloc(&e.w, bytes), "NTT expanded twiddle table allocation"));
+      k_expand_twiddles<<<grid_for(1ll << (lr + ls), 128), 128, 0, s>>>(f, rt.t_lo, rt.t_hi, rt.s, rt.log_N,
+                                                                        lr, ls, inverse, e.w);
+      int rc = check_launch("NTT expanded twiddle table");
+      if (rc == ZKB_OK) rc = check_cuda(cudaStreamSynchronize(s), "NTT expanded twiddle table build");
       if (rc != ZKB_OK) {
         cudaFree(e.w);
         return rc;
@@ -763,6 +782,20 @@ static int lookup_full(const F& f, const TableKey& key, const RootTables& rt, in
       *t_full = e.w;
     }
   }
+  return ZKB_OK;
+}
+
+// The coset / inverse scale factors of a transform of n = 2^log_n rows, expanded
+// inside its scale entry (st->g_full; null when it does not fit the byte budget).
+template <class F>
+static int lookup_scale_full(const F& f, int64_t n, int log_n, ScaleTables* st, cudaStream_t s) {
+  const size_t budget = (size_t)tune_get("ntt.full_table_mb") << 20;
+  if (log_n < kMinFullLog || budget == 0) {
+    st->g_full = nullptr;  // a budget of 0 means the two-level tables, cached expansions or not
+    return ZKB_OK;
+  }
+  const size_t bytes = (size_t)n * 32;
+  std::lock_guard<std::mutex> lock(g_ntt_mutex);
   if (st->g_lo && !st->g_full && g_full_bytes + bytes <= budget) {
     for (ScaleEntry& e : g_scales) {
       if (e.t.g_lo != st->g_lo) continue;
@@ -897,8 +930,7 @@ static int run_ntt(const F& f, const zkb_field* field, const uint64_t* in, uint6
   RootTables rt;
   ScaleTables st;
   ZKB_TRY(lookup_tables(f, key, n, log_n, invert, coset, rt, st, s));
-  const uint64_t* t_full = nullptr;
-  ZKB_TRY(lookup_full(f, key, rt, n, log_n, &st, &t_full, s));
+  ZKB_TRY(lookup_scale_full(f, n, log_n, &st, s));
 
   const size_t need = workspace_bytes(n);
   if (need && (!workspace || ws_bytes < need)) {
@@ -912,8 +944,9 @@ static int run_ntt(const F& f, const zkb_field* field, const uint64_t* in, uint6
               0, passes);
   const int P = (int)passes.size();
   for (int q = 0; q < P; ++q) {
-    passes[q].a.t_full = t_full;
-    passes[q].a.full_shift = rt.log_N - log_n;
+    if (!passes[q].a.last) {
+      ZKB_TRY(lookup_twiddles(f, key, rt, passes[q].a.lr, passes[q].a.ls, invert, &passes[q].a.t_full, s));
+    }
     const PassLaunch& L = passes[q];
     auto kern = tune_get("ntt.call_products") ? k_ntt_pass<F, true> : k_ntt_pass<F, false>;
     ZKB_TRY(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
