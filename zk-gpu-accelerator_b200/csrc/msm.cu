@@ -426,9 +426,9 @@ __device__ __forceinline__ void acc_points(const MsmJobs& J, const uint32_t* key
   if (cur != none) sink.flush(cur, acc, first, true);
 }
 
-// One MSM (108 registers, four CTAs per SM).
+// One MSM: capped at 128 registers, four CTAs per SM.
 template <class M>
-__global__ void __launch_bounds__(128) k_msm_acc_points(const MsmJobs J, const uint32_t* keys,
+__global__ void __launch_bounds__(128, 4) k_msm_acc_points(const MsmJobs J, const uint32_t* keys,
                                                         const uint32_t* vals, int64_t E, int K,
                                                         uint32_t none, uint64_t* buckets,
                                                         uint32_t* slot_keys, uint64_t* slot_pts) {
