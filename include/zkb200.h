@@ -295,7 +295,9 @@ int zkb_msm_batch(const zkb_msm_job* jobs, int count, void* workspace, size_t wo
 
 /* Tuning knobs, read by each call when it plans its work (so they also change
  * the workspace size queries): "msm.pairs_per_thread" (default 64),
- * "msm.slots_per_thread" (8), "msm.reduce_log_segment" (2),
+ * "msm.slots_per_thread" (8), "msm.reduce_log_segment" (2), "msm.sort" (1:
+ * pairs grouped by a counting sort that skips zero digits; 0: a radix sort
+ * of all pairs; the same points either way),
  * "ntt.max_log_radix" (12, range 8..12: the largest sub-transform one NTT pass
  * does), "ntt.cta_log_elems" (log2 of the rows staged per NTT block, 9..12;
  * default 0 = 12 for large transforms, 10 when fewer than four 4096-row

@@ -139,6 +139,39 @@ def test_inlined_products_give_the_same_point(case):
         _native.tune_set("msm.call_products", 1)
 
 
+@pytest.mark.parametrize("sort", [0, 1], ids=["radix-sort", "counting-sort"])
+def test_both_pair_sorts_give_the_references_points(sort):
+    """The radix sort of all pairs (msm.sort = 0) and the counting sort that skips zero digits
+    (msm.sort = 1, the default) give the reference's points: the seeded uniform and skewed cases,
+    the bucket edge cases, a heavy bucket, boolean and all-zero scalars, and a batch."""
+    from zkgpu import batch
+
+    try:
+        _native.tune_set("msm.sort", sort)
+        for case in golden("msm.json")["seeded"][:2]:
+            n = case["n"]
+            bases = _bases(n, case["base_seed"])
+            gen = wl.uniform_fr if case["kind"] == "uniform" else wl.skewed_scalars
+            sc = gen(case["scalar_seed"], n)
+            for w in (None, 5, 16):
+                assert msm_pippenger_rows(bases, sc, window_size=w) == expected_point(case), (case["kind"], w)
+        test_bucket_edge_cases()
+        test_heavy_bucket_and_boolean_scalars()
+        pts = [po.scalar_mul(po.G, k) for k in range(1, 65)]
+        assert msm_pippenger_gpu([p[0] for p in pts], [p[1] for p in pts], [0] * 64) == Point.identity()
+        case = golden("msm.json")["seeded"][0]
+        bases = _bases(case["n"], case["base_seed"])
+        import torch
+
+        sc = torch.from_numpy(wl.uniform_fr(case["scalar_seed"], case["n"])).cuda()
+        zeros = torch.zeros_like(sc)
+        got = batch.msm_batch([bases, bases[:100], bases], [sc, sc[:100], zeros])
+        assert got[0] == expected_point(case) and got[2] == Point.identity()
+        assert got[1] == msm_pippenger_rows(bases[:100], sc[:100])
+    finally:
+        _native.tune_set("msm.sort", 1)
+
+
 def test_self_test_passes():
     msm_gpu.compile_kernels()
 

@@ -7,9 +7,14 @@
 //                w-bit digits d (|d| <= 2^(w-1)), and emit one (bucket, point)
 //                pair per nonzero digit: key = window * 2^(w-1) + |d| - 1,
 //                value = point index | sign << 31.
-//   2. sort      radix sort of the pairs by key (CUB onesweep), so every
-//                bucket's points are contiguous; zero digits carry the largest
-//                key and sort to the end.
+//   2. sort      group the pairs by key, so every bucket's points are
+//                contiguous: either a counting sort ("msm.sort" = 1): the
+//                digits pass counts each key (warp-aggregated atomics, zero
+//                digits skipped), a scan turns counts into bucket offsets, and
+//                a second digits pass scatters each pair into its bucket's
+//                range; or a radix sort of all 2 W n pairs by key (CUB
+//                onesweep, "msm.sort" = 0), zero digits carrying the largest
+//                key and sorting to the end.
 //   3. buckets   level 1: each thread adds a fixed run of K1 sorted pairs into
 //                XYZZ accumulators with mixed additions, so every thread does
 //                the same work however skewed the buckets are. A bucket wholly
@@ -28,6 +33,7 @@
 //   sum_b (b + delta) X_b = sum_t U_t + L * sum_t t S_t,
 // and the last term is the same problem on the L S_t with delta = 0.
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include <algorithm>
 #include <cstring>
@@ -302,6 +308,70 @@ __global__ void __launch_bounds__(256) k_msm_digits(const MsmJobs J, int w, int 
   }
 }
 
+// Counting sort of the pairs (no entry for a zero digit). One thread per scalar,
+// a warp at a time: lanes whose digits fall in the same bucket take one atomic
+// together (__match_any_sync), so a bucket that most scalars share (skewed
+// scalars: digit 1 of window 0) costs one atomic per warp, not per lane.
+// kScatter = false: count[key] += pairs. kScatter = true: each pair takes the
+// next slot of its bucket, cursor[key]++ (the cursors start at the bucket
+// offsets), and is written there as one 8-byte (key, value) word. Within a bucket the order of the pairs
+// varies from run to run; the bucket sum, and so the result, does not.
+template <bool kScatter>
+__global__ void __launch_bounds__(256) k_msm_bucket_digits(const MsmJobs J, int w, int W, uint32_t none,
+                                                           uint32_t* ctr, uint2* pairs) {
+  FrP fr;
+  const int64_t N = J.first[J.count];
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;  // a multiple of 32
+  const int lane = threadIdx.x & 31;
+  const uint32_t half = 1u << (w - 1);
+  for (int64_t g0 = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); g0 < N; g0 += stride) {
+    const int64_t g = g0 + lane;  // the whole warp runs every iteration; lanes past N have no digits
+    uint32_t k[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}}, neg[2] = {0, 0};
+    int64_t n = 0, i = 0;
+    uint32_t key_base = 0;
+    if (g < N) {
+      const int j = job_of_point(J, g);
+      n = J.first[j + 1] - J.first[j];
+      i = g - J.first[j];
+      key_base = (uint32_t)j * J.keys_per_job;
+      uint32_t sc[8];
+      fe_load_nc(sc, J.scalars[j] + 4 * i);
+      fe_reduce_full(sc, fr, 5);
+      glv_split(sc, k[0], neg[0], k[1], neg[1]);
+    }
+    for (int h = 0; h < 2; ++h) {
+      const uint32_t point = (uint32_t)(h ? n + i : i);
+      uint32_t carry = 0;
+      for (int win = 0; win < W; ++win) {
+        const uint32_t raw = half_bits(k[h], win * w, w) + carry;
+        uint32_t mag, dneg = 0;
+        if (win + 1 < W && raw > half) {
+          mag = (1u << w) - raw;
+          dneg = 1;
+          carry = 1;
+        } else {
+          mag = raw;
+          carry = 0;
+        }
+        const uint32_t key = mag ? key_base + (((uint32_t)win << (w - 1)) | (mag - 1)) : none;
+        const unsigned peers = __match_any_sync(0xffffffffu, key);
+        const int leader = __ffs(peers) - 1;
+        if (!kScatter) {
+          if (lane == leader && key != none) atomicAdd(ctr + key, (uint32_t)__popc(peers));
+        } else {
+          uint32_t base = 0;
+          if (lane == leader && key != none) base = atomicAdd(ctr + key, (uint32_t)__popc(peers));
+          base = __shfl_sync(0xffffffffu, base, leader);
+          if (key != none) {
+            const uint32_t pos = base + (uint32_t)__popc(peers & ((1u << lane) - 1u));
+            pairs[pos] = make_uint2(key, point | ((neg[h] ^ dneg) << 31));
+          }
+        }
+      }
+    }
+  }
+}
+
 // phi(P_i) = (beta x_i, y_i), the points that the k2 halves multiply.
 __global__ void __launch_bounds__(256) k_msm_phi(const MsmJobs J) {
   FqP f;
@@ -387,27 +457,33 @@ __device__ __forceinline__ JobPoints job_points(const MsmJobs& J, uint32_t key) 
 // Level 1: K1 sorted (key, value) pairs per thread, mixed additions of affine
 // input points. kBatch = false is the one-job form: the job lookup at each
 // new run costs 40+ registers, so a single MSM keeps its point arrays fixed.
+// E_dev (null for the radix sort): the number of pairs the counting sort wrote,
+// at most E; the threads past it only clear their slots. Pair e is
+// (keys[e st], vals[e st]): st = 1 for the radix sort's two arrays, 2 for the
+// counting sort's interleaved (key, value) words.
 template <bool kBatch, class M>
 __device__ __forceinline__ void acc_points(const MsmJobs& J, const uint32_t* keys,
-                                           const uint32_t* vals, int64_t E, int K, uint32_t none,
-                                           uint64_t* buckets, uint32_t* slot_keys,
+                                           const uint32_t* vals, int st, int64_t E, const uint32_t* E_dev,
+                                           int K, uint32_t none, uint64_t* buckets, uint32_t* slot_keys,
                                            uint64_t* slot_pts) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t T = (E + K - 1) / K;
   if (t >= T) return;
-  const int64_t start = t * K;
-  const int64_t end = start + K < E ? start + K : E;
-  RunSink sink{buckets, slot_keys, slot_pts, t, start > 0 ? keys[start - 1] : none,
-               end < E ? keys[end] : none, none};
   slot_keys[2 * t] = none;
   slot_keys[2 * t + 1] = none;
-  uint32_t cur = keys[start];
+  if (E_dev) E = *E_dev;
+  const int64_t start = t * K;
+  if (start >= E) return;
+  const int64_t end = start + K < E ? start + K : E;
+  RunSink sink{buckets, slot_keys, slot_pts, t, start > 0 ? keys[(start - 1) * st] : none,
+               end < E ? keys[end * st] : none, none};
+  uint32_t cur = keys[start * st];
   bool first = true;
   Xyzz acc;
   xyzz_set_identity(acc);
   JobPoints jp = job_points(J, (!kBatch || cur == none) ? 0 : cur);
   for (int64_t e = start; e < end; ++e) {
-    const uint32_t k = keys[e];
+    const uint32_t k = keys[e * st];
     if (k != cur) {
       sink.flush(cur, acc, first, false);
       first = false;
@@ -416,7 +492,7 @@ __device__ __forceinline__ void acc_points(const MsmJobs& J, const uint32_t* key
       if (kBatch && k != none) jp = job_points(J, k);
     }
     if (k == none) break;  // zero digits sort last: nothing after them
-    const uint32_t v = vals[e];
+    const uint32_t v = vals[e * st];
     const int64_t idx = (int64_t)(v & 0x7fffffffu);
     Aff q;
     aff_load_nc(q, idx < jp.n ? jp.points + 8 * idx : jp.phi + 8 * (idx - jp.n));
@@ -429,10 +505,11 @@ __device__ __forceinline__ void acc_points(const MsmJobs& J, const uint32_t* key
 // One MSM: capped at 128 registers, four CTAs per SM.
 template <class M>
 __global__ void __launch_bounds__(128, 4) k_msm_acc_points(const MsmJobs J, const uint32_t* keys,
-                                                        const uint32_t* vals, int64_t E, int K,
-                                                        uint32_t none, uint64_t* buckets,
-                                                        uint32_t* slot_keys, uint64_t* slot_pts) {
-  acc_points<false, M>(J, keys, vals, E, K, none, buckets, slot_keys, slot_pts);
+                                                        const uint32_t* vals, int st, int64_t E,
+                                                        const uint32_t* E_dev, int K, uint32_t none,
+                                                        uint64_t* buckets, uint32_t* slot_keys,
+                                                        uint64_t* slot_pts) {
+  acc_points<false, M>(J, keys, vals, st, E, E_dev, K, none, buckets, slot_keys, slot_pts);
 }
 
 // A batch: capped at 128 registers (a few bytes of spill on the job-change
@@ -440,12 +517,12 @@ __global__ void __launch_bounds__(128, 4) k_msm_acc_points(const MsmJobs J, cons
 template <class M>
 __global__ void __launch_bounds__(128, 4) k_msm_acc_points_batch(const MsmJobs J,
                                                                  const uint32_t* keys,
-                                                                 const uint32_t* vals, int64_t E,
-                                                                 int K, uint32_t none,
-                                                                 uint64_t* buckets,
+                                                                 const uint32_t* vals, int st, int64_t E,
+                                                                 const uint32_t* E_dev, int K,
+                                                                 uint32_t none, uint64_t* buckets,
                                                                  uint32_t* slot_keys,
                                                                  uint64_t* slot_pts) {
-  acc_points<true, M>(J, keys, vals, E, K, none, buckets, slot_keys, slot_pts);
+  acc_points<true, M>(J, keys, vals, st, E, E_dev, K, none, buckets, slot_keys, slot_pts);
 }
 
 // Levels 2+: K2 slots per thread, full XYZZ additions; slots without a key
@@ -615,6 +692,8 @@ struct MsmPlan {
   int k2 = 8;      // slots per merge thread ("msm.slots_per_thread")
   int log_l = 2;   // log2 running-sum segment ("msm.reduce_log_segment")
   int call_products = 1;  // bucket kernels call one shared product ("msm.call_products")
+  int counting_sort = 1;  // counting sort (1) or radix sort (0) of the pairs ("msm.sort")
+  int64_t keys_used = 0;  // bucket keys of the batch (count * W * 2^(w-1))
   int64_t E = 0;   // sorted pairs
   int64_t T1 = 0;  // level-1 threads
   std::vector<int64_t> slot_levels;  // thread count of each merge level
@@ -622,7 +701,7 @@ struct MsmPlan {
   // workspace offsets
   size_t off_keys0, off_keys1, off_vals0, off_vals1, off_cub, off_phi, off_buckets,
       off_slot_keys_a, off_slot_pts_a, off_slot_keys_b, off_slot_pts_b, off_red_s0, off_red_u0,
-      off_red_s1, off_red_u1, off_wsum, total;
+      off_red_s1, off_red_u1, off_wsum, off_counts, off_offsets, total;
 };
 
 // Plan for a batch of jobs with point counts sizes[0..count) at window w.
@@ -640,6 +719,8 @@ static int make_plan(const int64_t* sizes, int count, int w, MsmPlan& p) {
   while ((1ll << bits) <= keys_used) ++bits;  // keys_used itself must fit below none
   p.key_bits = bits;
   p.none = (uint32_t)((1ull << bits) - 1);
+  p.keys_used = keys_used;
+  p.counting_sort = tune_get("msm.sort");
   p.E = 2 * (int64_t)p.W * n;  // both GLV halves
   p.k1 = tune_get("msm.pairs_per_thread");
   p.k2 = tune_get("msm.slots_per_thread");
@@ -660,7 +741,11 @@ static int make_plan(const int64_t* sizes, int count, int w, MsmPlan& p) {
   cudaError_t err = cub::DeviceRadixSort::SortPairs(nullptr, cub_bytes, kb, vb, (int)p.E, 0,
                                                     p.key_bits, (cudaStream_t)0);
   if (err != cudaSuccess) return check_cuda(err, "CUB sort size query");
-  p.cub_bytes = cub_bytes;
+  size_t scan_bytes = 0;
+  err = cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (const uint32_t*)nullptr, (uint32_t*)nullptr,
+                                      (int)(keys_used + 1), (cudaStream_t)0);
+  if (err != cudaSuccess) return check_cuda(err, "CUB scan size query");
+  p.cub_bytes = cub_bytes > scan_bytes ? cub_bytes : scan_bytes;
 
   size_t off = 0;
   auto take = [&](size_t bytes) {
@@ -687,6 +772,9 @@ static int make_plan(const int64_t* sizes, int count, int w, MsmPlan& p) {
   p.off_red_s1 = take((size_t)red * 128);
   p.off_red_u1 = take((size_t)red * 128);
   p.off_wsum = take((size_t)windows * 128);
+  // counting sort: per-key counts, then offsets / cursors (one more entry: the total)
+  p.off_counts = take((size_t)(keys_used + 1) * 4);
+  p.off_offsets = take((size_t)(keys_used + 1) * 4);
   p.total = off;
   return ZKB_OK;
 }
@@ -717,26 +805,53 @@ static int run_msm(const MsmJobs& J, const MsmPlan& p, char* ws, cudaStream_t s)
   uint64_t* buckets = reinterpret_cast<uint64_t*>(ws + p.off_buckets);
   const int64_t windows = (int64_t)p.count * p.W;
 
-  // 1. digits (GLV halves) and the phi images of the points
-  {
-    ProfSpan span("msm_digits", s);
-    k_msm_digits<<<grid_for(p.n, 256), 256, 0, s>>>(J, p.w, p.W, p.none, keys0, vals0);
-    ZKB_TRY(check_launch("msm digits"));
-    k_msm_phi<<<grid_for(p.n, 256), 256, 0, s>>>(J);
-    ZKB_TRY(check_launch("msm phi points"));
-  }
-
-  // 2. sort
-  cub::DoubleBuffer<uint32_t> kb(keys0, keys1), vb(vals0, vals1);
-  size_t cub_bytes = p.cub_bytes;
-  {
+  // 1-2. digits (GLV halves), grouped by bucket; the phi images of the points
+  const uint32_t* skeys = keys1;
+  const uint32_t* svals = vals1;
+  int st = 1;
+  const uint32_t* e_dev = nullptr;  // pairs written by the counting sort (device)
+  if (p.counting_sort) {
+    uint32_t* counts = reinterpret_cast<uint32_t*>(ws + p.off_counts);
+    uint32_t* offsets = reinterpret_cast<uint32_t*>(ws + p.off_offsets);
+    {
+      ProfSpan span("msm_digits", s);
+      ZKB_TRY(check_cuda(cudaMemsetAsync(counts, 0, (size_t)(p.keys_used + 1) * 4, s), "msm count reset"));
+      k_msm_bucket_digits<false><<<grid_for(p.n, 256), 256, 0, s>>>(J, p.w, p.W, p.none, counts, nullptr);
+      ZKB_TRY(check_launch("msm digit count"));
+      k_msm_phi<<<grid_for(p.n, 256), 256, 0, s>>>(J);
+      ZKB_TRY(check_launch("msm phi points"));
+    }
+    ProfSpan span("msm_sort", s);
+    size_t scan_bytes = p.cub_bytes;
+    ZKB_TRY(check_cuda(cub::DeviceScan::ExclusiveSum(ws + p.off_cub, scan_bytes, counts, offsets,
+                                                     (int)(p.keys_used + 1), s),
+                       "msm bucket offsets"));
+    // offsets[keys_used] = the pair count; no key reaches it, so it survives the scatter
+    // the interleaved (key, value) words take the space of keys0 and keys1 (2 x 4 E bytes)
+    uint2* pairs = reinterpret_cast<uint2*>(keys0);
+    k_msm_bucket_digits<true><<<grid_for(p.n, 256), 256, 0, s>>>(J, p.w, p.W, p.none, offsets, pairs);
+    ZKB_TRY(check_launch("msm digit scatter"));
+    e_dev = offsets + p.keys_used;
+    skeys = keys0;
+    svals = keys0 + 1;
+    st = 2;
+  } else {
+    {
+      ProfSpan span("msm_digits", s);
+      k_msm_digits<<<grid_for(p.n, 256), 256, 0, s>>>(J, p.w, p.W, p.none, keys0, vals0);
+      ZKB_TRY(check_launch("msm digits"));
+      k_msm_phi<<<grid_for(p.n, 256), 256, 0, s>>>(J);
+      ZKB_TRY(check_launch("msm phi points"));
+    }
+    cub::DoubleBuffer<uint32_t> kb(keys0, keys1), vb(vals0, vals1);
+    size_t cub_bytes = p.cub_bytes;
     ProfSpan span("msm_sort", s);
     ZKB_TRY(check_cuda(cub::DeviceRadixSort::SortPairs(ws + p.off_cub, cub_bytes, kb, vb, (int)p.E,
                                                        0, p.key_bits, s),
                        "msm sort"));
+    skeys = kb.Current();
+    svals = vb.Current();
   }
-  const uint32_t* skeys = kb.Current();
-  const uint32_t* svals = vb.Current();
 
   // 3. buckets
   const int64_t nbuckets = windows * p.nb;
@@ -751,10 +866,10 @@ static int run_msm(const MsmJobs& J, const MsmPlan& p, char* ws, cudaStream_t s)
     const unsigned grid = (unsigned)((p.T1 + 127) / 128);
     if (p.count > 1) {
       auto kern = p.call_products ? k_msm_acc_points_batch<CallMul> : k_msm_acc_points_batch<InlineMul>;
-      kern<<<grid, 128, 0, s>>>(J, skeys, svals, p.E, p.k1, p.none, buckets, sk[0], sp[0]);
+      kern<<<grid, 128, 0, s>>>(J, skeys, svals, st, p.E, e_dev, p.k1, p.none, buckets, sk[0], sp[0]);
     } else {
       auto kern = p.call_products ? k_msm_acc_points<CallMul> : k_msm_acc_points<InlineMul>;
-      kern<<<grid, 128, 0, s>>>(J, skeys, svals, p.E, p.k1, p.none, buckets, sk[0], sp[0]);
+      kern<<<grid, 128, 0, s>>>(J, skeys, svals, st, p.E, e_dev, p.k1, p.none, buckets, sk[0], sp[0]);
     }
     ZKB_TRY(check_launch("msm bucket accumulation"));
   }
