@@ -106,3 +106,19 @@ def test_no_cpu_fallback_without_a_device():
         field_gpu.gpu_batch_mul(x, x, 7)
     with pytest.raises(RuntimeError, match="no CPU fallback"):
         ntt_gpu(x, 998_244_353)
+
+
+def test_ntt64_c_abi_refuses_overlapping_buffers():
+    """zkb_ntt64 gathers its input in bit-reversed order, so in and out must not overlap: the
+    C ABI refuses it before any device work (addresses only; skipped where a GPU is visible,
+    so that no kernel could ever see these stand-in pointers)."""
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is visible")
+    from zkgpu import _native
+
+    lib = _native.lib()
+    base = 1 << 20
+    for out in (base, base + 8, base + 24):
+        rc = lib.zkb_ntt64(base, out, 4, 998_244_353, 911_660_635, 0, base + 4096, 1 << 16, None)
+        assert rc == 1 and "overlap" in _native.last_error()
