@@ -809,19 +809,28 @@ def run_int64(log_n: int = 25, log_ops: int = 26, cpu: bool = True) -> dict:
     return out
 
 
-def run_served(n_jobs: int = 2000, rate: float = 200.0, log_max: int = 20, seed: int = 7) -> dict:
+def run_served(n_jobs: int = 2000, rate: float = 200.0, log_max: int = 20, seed: int = 7,
+               table_window: int = 16) -> dict:
     """Poisson stream (rate jobs/s) of Groth16-shaped jobs, m = 2^U{12..log_max}: each job 3
     inverse NTTs, 3 coset NTTs, the pointwise quotient, 1 inverse coset NTT and 4 G1 MSMs
     (skewed witness scalars; h for the last) over a resident base set. The served form
-    (zkgpu.serving) against the same jobs one at a time (prove_plain, a 60-job sample)."""
+    (zkgpu.serving) against the same jobs one at a time (prove_plain, a 60-job sample). The
+    base set stays resident, as a prover's SRS does, so both forms run their MSMs over one
+    fixed-base table of it (table_window; 0 = the plain MSM), built once before either runs."""
     import numpy as np
     import torch
 
     from zkgpu import curve_gpu, workloads as wl
+    from zkgpu.msm_gpu import FixedBaseTable
     from zkgpu.prover import ProofJob, prove_plain, synthetic_request
     from zkgpu.serving import Server, summarize
 
     bases = curve_gpu.mul_generator(wl.base_scalars(seed, 1 << log_max))
+    torch.cuda.synchronize()
+    t_build = time.perf_counter()
+    table = FixedBaseTable(bases, table_window) if table_window else None
+    torch.cuda.synchronize()
+    t_build = (time.perf_counter() - t_build) * 1e3
     pool = {1 << e: [synthetic_request(1000 * e + k, 1 << e) for k in range(2)] for e in range(12, log_max + 1)}
     rng = np.random.default_rng(seed)
     exps = rng.integers(12, log_max + 1, size=n_jobs)
@@ -833,23 +842,23 @@ def run_served(n_jobs: int = 2000, rate: float = 200.0, log_max: int = 20, seed:
     sample = reqs[: min(60, n_jobs)]
     ws: dict = {}
     for r in sample[:3]:
-        prove_plain(ProofJob(r, bases), ws)
+        prove_plain(ProofJob(r, bases), ws, table)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for r in sample:
-        prove_plain(ProofJob(r, bases), ws)
+        prove_plain(ProofJob(r, bases), ws, table)
         torch.cuda.synchronize()
     plain_s = time.perf_counter() - t0
     budget = 60 << 30
-    Server(bases, budget).run(sample[:10], [0.0] * 10)  # warm-up: tables, allocator
-    srv = Server(bases, budget)
+    Server(bases, budget, table=table).run(sample[:10], [0.0] * 10)  # warm-up: tables, allocator
+    srv = Server(bases, budget, table=table)
     t0 = time.perf_counter()
     recs = srv.run(reqs, list(arrivals))
     wall = time.perf_counter() - t0
     s = summarize(recs, wall)
     plain_jobs_s = len(sample) / plain_s
     # capacity: the first 200 jobs all queued at once (closed loop)
-    cap = Server(bases, budget)
+    cap = Server(bases, budget, table=table)
     t0 = time.perf_counter()
     cap_recs = cap.run(reqs[:200], [0.0] * min(200, n_jobs))
     cap_s = summarize(cap_recs, time.perf_counter() - t0)
@@ -866,6 +875,9 @@ def run_served(n_jobs: int = 2000, rate: float = 200.0, log_max: int = 20, seed:
         "plain": f"the first {len(sample)} jobs one at a time (one call per NTT / MSM, synchronised per job)",
         "ticks": srv.ticks, "gpu_launches": srv.launches, "hbm_budget_bytes": budget,
         "latency": "arrival (host clock) to the device-side completion of the job's last MSM batch",
+        "msm": (f"over a fixed-base table of the resident base set (w = {table_window}, "
+                f"{table.nbytes >> 20} MiB, built once in {t_build:.0f} ms), served and plain alike")
+               if table is not None else "zkb_msm_batch / zkb_msm over the base set",
     }
 
 

@@ -291,6 +291,35 @@ size_t zkb_msm_batch_workspace_bytes(const zkb_msm_job* jobs, int count);
 int zkb_msm_batch(const zkb_msm_job* jobs, int count, void* workspace, size_t workspace_bytes,
                   void* stream);
 
+/* ---- MSMs over a resident base set (fixed-base tables) ------------------- */
+
+/* These have no counterpart in the reference, whose MSM takes its points with
+ * every call. A prover that runs many MSMs over one resident base set (an SRS)
+ * builds a table once: for each point P_i its 2 W rows 2^(w win) P_i and
+ * phi(2^(w win) P_i), win < W = ceil(128 / w), affine Montgomery (64 bytes a
+ * row). An MSM over the table adds every window's digits into one set of
+ * 2^(w-1) buckets: fewer buckets to reduce, no doublings in the final
+ * combination, and room for larger windows, i.e. fewer mixed additions. The
+ * result equals zkb_msm's over the same points at any window. */
+
+/* Device bytes of the table of n points at window w (8..24): n * 2W * 64;
+ * 0 for an invalid window or n <= 0. */
+size_t zkb_msm_table_bytes(int64_t n, int window_size);
+
+/* Builds the table of `points` ((n, 2, 4) affine Montgomery rows on the curve,
+ * not the identity) at window w (8..24) into `table` (zkb_msm_table_bytes).
+ * A table of N points also serves every prefix of them: its first n * 2W rows
+ * are the table of the first n points. */
+int zkb_msm_table_build(const uint64_t* points, int64_t n, int window_size, uint64_t* table,
+                        void* stream);
+
+/* zkb_msm_batch over tables: jobs[j].points is a table built at window
+ * jobs[j].window_size (required, 8..24) of at least jobs[j].n points, and the
+ * job sums s_i P_i over its first n points. Results as zkb_msm_batch's. */
+size_t zkb_msm_fixed_batch_workspace_bytes(const zkb_msm_job* jobs, int count);
+int zkb_msm_fixed_batch(const zkb_msm_job* jobs, int count, void* workspace, size_t workspace_bytes,
+                        void* stream);
+
 /* ---- measurement -------------------------------------------------------- */
 
 /* Tuning knobs, read by each call when it plans its work (so they also change

@@ -226,6 +226,7 @@ struct MsmJobs {
   const uint64_t* scalars[kMsmMaxBatch];
   uint64_t* phi[kMsmMaxBatch];        // phi images, in the workspace
   uint64_t* result[kMsmMaxBatch];
+  int64_t pts_n[kMsmMaxBatch];        // rows of points[j]: n_j, or n_j 2 W for a fixed-base table
 };
 
 // The job holding batch-wide point index i (first[j] <= i < first[j + 1]).
@@ -316,9 +317,12 @@ __global__ void __launch_bounds__(256) k_msm_digits(const MsmJobs J, int w, int 
 // next slot of its bucket, cursor[key]++ (the cursors start at the bucket
 // offsets), and is written there as one 8-byte (key, value) word. Within a bucket the order of the pairs
 // varies from run to run; the bucket sum, and so the result, does not.
+// With a fixed-base table (table = 1) every window shares the job's one set of
+// 2^(w-1) buckets: key = |d| - 1, and the value names the table row of
+// 2^(w win) P (or of its phi image), (point 2 + half) W + win.
 template <bool kScatter>
 __global__ void __launch_bounds__(256) k_msm_bucket_digits(const MsmJobs J, int w, int W, uint32_t none,
-                                                           uint32_t* ctr, uint2* pairs) {
+                                                           int table, uint32_t* ctr, uint2* pairs) {
   FrP fr;
   const int64_t N = J.first[J.count];
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;  // a multiple of 32
@@ -353,7 +357,8 @@ __global__ void __launch_bounds__(256) k_msm_bucket_digits(const MsmJobs J, int 
           mag = raw;
           carry = 0;
         }
-        const uint32_t key = mag ? key_base + (((uint32_t)win << (w - 1)) | (mag - 1)) : none;
+        const uint32_t key =
+            mag ? key_base + (table ? mag - 1 : (((uint32_t)win << (w - 1)) | (mag - 1))) : none;
         const unsigned peers = __match_any_sync(0xffffffffu, key);
         const int leader = __ffs(peers) - 1;
         if (!kScatter) {
@@ -364,7 +369,8 @@ __global__ void __launch_bounds__(256) k_msm_bucket_digits(const MsmJobs J, int 
           base = __shfl_sync(0xffffffffu, base, leader);
           if (key != none) {
             const uint32_t pos = base + (uint32_t)__popc(peers & ((1u << lane) - 1u));
-            pairs[pos] = make_uint2(key, point | ((neg[h] ^ dneg) << 31));
+            const uint32_t row = table ? (uint32_t)((2 * i + h) * W + win) : point;
+            pairs[pos] = make_uint2(key, row | ((neg[h] ^ dneg) << 31));
           }
         }
       }
@@ -388,6 +394,69 @@ __global__ void __launch_bounds__(256) k_msm_phi(const MsmJobs J) {
     fe_mul(x, x, beta, f);
     fe_store(J.phi[j] + 8 * i, x);
     fe_store(J.phi[j] + 8 * i + 4, y);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Fixed-base tables (no counterpart in the reference, which takes its points
+// with every call). For a base set that stays resident across many MSMs, the
+// table holds per point P_i its 2 W rows 2^(w win) P_i and phi(2^(w win) P_i),
+// win < W, affine Montgomery, at rows (2 i + half) W + win. An MSM over the
+// table adds every window's digits into one set of 2^(w-1) buckets, so a job
+// reduces one window and its final combination needs no doublings; the
+// smaller bucket work allows larger windows, i.e. fewer mixed additions.
+// ---------------------------------------------------------------------------
+
+static constexpr int kTableMinWindow = 8, kTableMaxWindow = 24;
+static constexpr int kTableMaxWindows = 16;  // ceil(128 / 8)
+
+// One thread per base point: the W multiples by w doublings each (XYZZ), one
+// inversion for all of them (prefix products of ZZ ZZZ), then x = X / ZZ,
+// y = Y / ZZZ and the phi images (beta x, y).
+__global__ void __launch_bounds__(128) k_msm_table_build(const uint64_t* points, int64_t n, int w, int W,
+                                                         uint64_t* table) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  G1F f;
+  uint32_t beta[8];
+  glv_beta_mont(beta);
+  Aff p;
+  aff_load_nc(p, points + 8 * i);
+  Xyzz m[kTableMaxWindows];
+  xyzz_from_affine(m[0], p);
+  for (int k = 1; k < W; ++k) {
+    m[k] = m[k - 1];
+    for (int d = 0; d < w; ++d) xyzz_dbl<CallMul>(m[k], m[k]);
+  }
+  uint32_t pre[kTableMaxWindows][8];  // pre[k] = prod_{t <= k} ZZ_t ZZZ_t
+  fe_mul(pre[0], m[0].zz, m[0].zzz, f);
+  for (int k = 1; k < W; ++k) {
+    uint32_t t[8];
+    fe_mul(t, m[k].zz, m[k].zzz, f);
+    fe_mul(pre[k], pre[k - 1], t, f);
+  }
+  uint32_t inv[8];  // 1 / pre[k], walking down
+  fe_inv(inv, pre[W - 1], f);
+  for (int k = W - 1; k >= 0; --k) {
+    uint32_t ik[8], t[8], x[8], y[8];
+    if (k > 0) {
+      fe_mul(ik, inv, pre[k - 1], f);  // 1 / (ZZ_k ZZZ_k)
+      fe_mul(t, m[k].zz, m[k].zzz, f);
+      fe_mul(inv, inv, t, f);          // 1 / pre[k - 1]
+    } else {
+      fe_copy(ik, inv);
+    }
+    fe_mul(t, ik, m[k].zzz, f);  // 1 / ZZ
+    fe_mul(x, m[k].x, t, f);
+    fe_mul(t, ik, m[k].zz, f);   // 1 / ZZZ
+    fe_mul(y, m[k].y, t, f);
+    uint64_t* row = table + 8 * ((2 * i) * W + k);
+    fe_store(row, x);
+    fe_store(row + 4, y);
+    fe_mul(x, x, beta, f);
+    row = table + 8 * ((2 * i + 1) * W + k);
+    fe_store(row, x);
+    fe_store(row + 4, y);
   }
 }
 
@@ -451,7 +520,7 @@ struct JobPoints {
 
 __device__ __forceinline__ JobPoints job_points(const MsmJobs& J, uint32_t key) {
   const int j = (int)(key / J.keys_per_job);
-  return JobPoints{J.points[j], J.phi[j], J.first[j + 1] - J.first[j]};
+  return JobPoints{J.points[j], J.phi[j], J.pts_n[j]};
 }
 
 // Level 1: K1 sorted (key, value) pairs per thread, mixed additions of affine
@@ -693,6 +762,8 @@ struct MsmPlan {
   int log_l = 2;   // log2 running-sum segment ("msm.reduce_log_segment")
   int call_products = 1;  // bucket kernels call one shared product ("msm.call_products")
   int counting_sort = 1;  // counting sort (1) or radix sort (0) of the pairs ("msm.sort")
+  int table = 0;          // points are fixed-base tables: one bucket set per job
+  int64_t windows = 0;    // bucket sets of the batch: count W, or count with tables
   int64_t keys_used = 0;  // bucket keys of the batch (count * W * 2^(w-1))
   int64_t E = 0;   // sorted pairs
   int64_t T1 = 0;  // level-1 threads
@@ -705,7 +776,7 @@ struct MsmPlan {
 };
 
 // Plan for a batch of jobs with point counts sizes[0..count) at window w.
-static int make_plan(const int64_t* sizes, int count, int w, MsmPlan& p) {
+static int make_plan(const int64_t* sizes, int count, int w, MsmPlan& p, int table = 0) {
   p.count = count;
   p.first.assign(count + 1, 0);
   for (int j = 0; j < count; ++j) p.first[j + 1] = p.first[j] + sizes[j];
@@ -714,13 +785,15 @@ static int make_plan(const int64_t* sizes, int count, int w, MsmPlan& p) {
   p.w = w;
   p.W = num_windows(w);
   p.nb = 1ll << (w - 1);
-  const int64_t keys_used = (int64_t)count * p.W * p.nb;
+  p.table = table;
+  p.windows = table ? count : (int64_t)count * p.W;
+  const int64_t keys_used = p.windows * p.nb;
   int bits = 1;
   while ((1ll << bits) <= keys_used) ++bits;  // keys_used itself must fit below none
   p.key_bits = bits;
   p.none = (uint32_t)((1ull << bits) - 1);
   p.keys_used = keys_used;
-  p.counting_sort = tune_get("msm.sort");
+  p.counting_sort = table ? 1 : tune_get("msm.sort");
   p.E = 2 * (int64_t)p.W * n;  // both GLV halves
   p.k1 = tune_get("msm.pairs_per_thread");
   p.k2 = tune_get("msm.slots_per_thread");
@@ -758,8 +831,8 @@ static int make_plan(const int64_t* sizes, int count, int w, MsmPlan& p) {
   p.off_vals0 = take((size_t)p.E * 4);
   p.off_vals1 = take((size_t)p.E * 4);
   p.off_cub = take(p.cub_bytes);
-  p.off_phi = take((size_t)n * 64);
-  const int64_t windows = (int64_t)count * p.W;  // the batch's windows
+  p.off_phi = take(table ? 0 : (size_t)n * 64);
+  const int64_t windows = p.windows;
   p.off_buckets = take((size_t)windows * p.nb * 128);
   p.off_slot_keys_a = take((size_t)2 * p.T1 * 4);
   p.off_slot_pts_a = take((size_t)2 * p.T1 * 128);
@@ -785,14 +858,15 @@ static MsmJobs job_table(const MsmPlan& p, const uint64_t* const* points,
   MsmJobs J;
   std::memset(&J, 0, sizeof J);
   J.count = p.count;
-  J.keys_per_job = (uint32_t)(p.W * p.nb);
+  J.keys_per_job = (uint32_t)(p.windows / p.count * p.nb);
   uint64_t* phi = reinterpret_cast<uint64_t*>(ws + p.off_phi);
   for (int j = 0; j <= p.count; ++j) J.first[j] = p.first[j];
   for (int j = 0; j < p.count; ++j) {
     J.points[j] = points[j];
     J.scalars[j] = scalars[j];
     J.result[j] = results[j];
-    J.phi[j] = phi + 8 * p.first[j];
+    J.phi[j] = p.table ? nullptr : phi + 8 * p.first[j];
+    J.pts_n[j] = (p.first[j + 1] - p.first[j]) * (p.table ? 2 * p.W : 1);
   }
   return J;
 }
@@ -803,7 +877,7 @@ static int run_msm(const MsmJobs& J, const MsmPlan& p, char* ws, cudaStream_t s)
   uint32_t* vals0 = reinterpret_cast<uint32_t*>(ws + p.off_vals0);
   uint32_t* vals1 = reinterpret_cast<uint32_t*>(ws + p.off_vals1);
   uint64_t* buckets = reinterpret_cast<uint64_t*>(ws + p.off_buckets);
-  const int64_t windows = (int64_t)p.count * p.W;
+  const int64_t windows = p.windows;
 
   // 1-2. digits (GLV halves), grouped by bucket; the phi images of the points
   const uint32_t* skeys = keys1;
@@ -816,10 +890,13 @@ static int run_msm(const MsmJobs& J, const MsmPlan& p, char* ws, cudaStream_t s)
     {
       ProfSpan span("msm_digits", s);
       ZKB_TRY(check_cuda(cudaMemsetAsync(counts, 0, (size_t)(p.keys_used + 1) * 4, s), "msm count reset"));
-      k_msm_bucket_digits<false><<<grid_for(p.n, 256), 256, 0, s>>>(J, p.w, p.W, p.none, counts, nullptr);
+      k_msm_bucket_digits<false><<<grid_for(p.n, 256), 256, 0, s>>>(J, p.w, p.W, p.none, p.table, counts,
+                                                                     nullptr);
       ZKB_TRY(check_launch("msm digit count"));
-      k_msm_phi<<<grid_for(p.n, 256), 256, 0, s>>>(J);
-      ZKB_TRY(check_launch("msm phi points"));
+      if (!p.table) {
+        k_msm_phi<<<grid_for(p.n, 256), 256, 0, s>>>(J);
+        ZKB_TRY(check_launch("msm phi points"));
+      }
     }
     ProfSpan span("msm_sort", s);
     size_t scan_bytes = p.cub_bytes;
@@ -829,7 +906,8 @@ static int run_msm(const MsmJobs& J, const MsmPlan& p, char* ws, cudaStream_t s)
     // offsets[keys_used] = the pair count; no key reaches it, so it survives the scatter
     // the interleaved (key, value) words take the space of keys0 and keys1 (2 x 4 E bytes)
     uint2* pairs = reinterpret_cast<uint2*>(keys0);
-    k_msm_bucket_digits<true><<<grid_for(p.n, 256), 256, 0, s>>>(J, p.w, p.W, p.none, offsets, pairs);
+    k_msm_bucket_digits<true><<<grid_for(p.n, 256), 256, 0, s>>>(J, p.w, p.W, p.none, p.table, offsets,
+                                                                  pairs);
     ZKB_TRY(check_launch("msm digit scatter"));
     e_dev = offsets + p.keys_used;
     skeys = keys0;
@@ -924,7 +1002,8 @@ static int run_msm(const MsmJobs& J, const MsmPlan& p, char* ws, cudaStream_t s)
   // 5. finalize
   ProfSpan fin_span("msm_finalize", s);
   auto fin = p.call_products ? k_msm_finalize<CallMul> : k_msm_finalize<InlineMul>;
-  fin<<<1, p.count < 32 ? 32 : p.count, 0, s>>>(J, wsum, p.W, p.w);
+  // with tables there is one window sum per job: nothing to combine
+  fin<<<1, p.count < 32 ? 32 : p.count, 0, s>>>(J, wsum, p.table ? 1 : p.W, p.w);
   return check_launch("msm finalize");
 }
 
@@ -940,10 +1019,10 @@ struct MsmChunk {
   size_t offset = 0;
 };
 
-static int validate_job(const zkb_msm_job& j, int index) {
+static int validate_job(const zkb_msm_job& j, int index, int table) {
   if (j.n < 0) return fail(ZKB_EINVAL, "job %d: negative point count", index);
   if (j.n >= (1ll << 30)) return fail(ZKB_EINVAL, "job %d: at most 2^30 - 1 points per MSM", index);
-  if (j.window_size < 0 || j.window_size > kMsmMaxWindow) {
+  if (!table && (j.window_size < 0 || j.window_size > kMsmMaxWindow)) {
     return fail(ZKB_EINVAL, "job %d: window_size must be in 1..%d (or 0 for the default), got %d",
                 index, kMsmMaxWindow, j.window_size);
   }
@@ -957,14 +1036,18 @@ static int validate_job(const zkb_msm_job& j, int index) {
 }
 
 static int plan_batch(const zkb_msm_job* jobs, int count, std::vector<MsmChunk>& chunks,
-                      size_t& total) {
+                      size_t& total, int table = 0) {
   chunks.clear();
   total = 0;
   if (count < 0) return fail(ZKB_EINVAL, "negative job count");
   if (count > 0 && !jobs) return fail(ZKB_EINVAL, "null job array");
   std::vector<int> order;
   for (int i = 0; i < count; ++i) {
-    ZKB_TRY(validate_job(jobs[i], i));
+    ZKB_TRY(validate_job(jobs[i], i, table));
+    if (table && (jobs[i].window_size < kTableMinWindow || jobs[i].window_size > kTableMaxWindow)) {
+      return fail(ZKB_EINVAL, "job %d: a fixed-base table's window must be %d..%d, got %d", i,
+                  kTableMinWindow, kTableMaxWindow, jobs[i].window_size);
+    }
     if (jobs[i].n > 0) order.push_back(i);
   }
   auto window_of = [&](int i) {
@@ -998,7 +1081,7 @@ static int plan_batch(const zkb_msm_job* jobs, int count, std::vector<MsmChunk>&
   for (auto& c : chunks) {
     std::vector<int64_t> sizes;
     for (int k : c.jobs) sizes.push_back(jobs[k].n);
-    ZKB_TRY(make_plan(sizes.data(), (int)sizes.size(), c.w, c.plan));
+    ZKB_TRY(make_plan(sizes.data(), (int)sizes.size(), c.w, c.plan, table));
     c.offset = total;
     total += align256(c.plan.total);
   }
@@ -1011,6 +1094,10 @@ static int run_single(const uint64_t* points, const uint64_t* scalars, uint64_t*
   const MsmJobs J = job_table(p, &points, &scalars, &result, ws);
   return run_msm(J, p, ws, s);
 }
+
+// A batch of MSM jobs (zkb_msm_batch), or of MSMs over fixed-base tables.
+int msm_batch(const zkb_msm_job* jobs, int count, void* workspace, size_t workspace_bytes, void* stream,
+              int table);
 
 }  // namespace zkb
 
@@ -1074,10 +1161,57 @@ size_t zkb_msm_batch_workspace_bytes(const zkb_msm_job* jobs, int count) {
 
 int zkb_msm_batch(const zkb_msm_job* jobs, int count, void* workspace, size_t workspace_bytes,
                   void* stream) {
+  return zkb::msm_batch(jobs, count, workspace, workspace_bytes, stream, 0);
+}
+
+size_t zkb_msm_table_bytes(int64_t n, int window_size) {
+  if (n <= 0 || window_size < kTableMinWindow || window_size > kTableMaxWindow) return 0;
+  return (size_t)n * 2 * num_windows(window_size) * 64;
+}
+
+int zkb_msm_table_build(const uint64_t* points, int64_t n, int window_size, uint64_t* table,
+                        void* stream) {
+  set_error("%s", "");
+  if (window_size < kTableMinWindow || window_size > kTableMaxWindow) {
+    return fail(ZKB_EINVAL, "a fixed-base table's window must be %d..%d, got %d", kTableMinWindow,
+                kTableMaxWindow, window_size);
+  }
+  const int W = num_windows(window_size);
+  if (n < 0 || n >= (1ll << 30) || 2 * (int64_t)W * n >= (1ll << 31)) {
+    return fail(ZKB_EINVAL, "%lld points do not fit a table at window %d", (long long)n, window_size);
+  }
+  if (n == 0) return ZKB_OK;
+  if (!points || !table) return fail(ZKB_EINVAL, "null buffer");
+  ZKB_TRY(check_align(points, 16, "points"));
+  ZKB_TRY(check_align(table, 16, "table"));
+  k_msm_table_build<<<(unsigned)((n + 127) / 128), 128, 0, as_stream(stream)>>>(points, n, window_size, W,
+                                                                                 table);
+  return check_launch("msm fixed-base table");
+}
+
+size_t zkb_msm_fixed_batch_workspace_bytes(const zkb_msm_job* jobs, int count) {
   set_error("%s", "");
   std::vector<MsmChunk> chunks;
   size_t total = 0;
-  ZKB_TRY(plan_batch(jobs, count, chunks, total));
+  if (plan_batch(jobs, count, chunks, total, 1) != ZKB_OK) return 0;
+  return total;
+}
+
+int zkb_msm_fixed_batch(const zkb_msm_job* jobs, int count, void* workspace, size_t workspace_bytes,
+                        void* stream) {
+  return zkb::msm_batch(jobs, count, workspace, workspace_bytes, stream, 1);
+}
+
+}  // extern "C"
+
+namespace zkb {
+
+int msm_batch(const zkb_msm_job* jobs, int count, void* workspace, size_t workspace_bytes, void* stream,
+              int table) {
+  set_error("%s", "");
+  std::vector<MsmChunk> chunks;
+  size_t total = 0;
+  ZKB_TRY(plan_batch(jobs, count, chunks, total, table));
   if (total > 0) {
     ZKB_TRY(check_align(workspace, 256, "workspace"));
     if (!workspace || workspace_bytes < total) {
@@ -1118,6 +1252,10 @@ int zkb_msm_batch(const zkb_msm_job* jobs, int count, void* workspace, size_t wo
   }
   return fan.join(s);
 }
+
+}  // namespace zkb
+
+extern "C" {
 
 }  // extern "C"
 

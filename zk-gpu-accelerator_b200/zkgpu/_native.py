@@ -122,6 +122,10 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "zkb_msm_no_alloc_capacity": (ctypes.c_size_t, []),
     "zkb_msm_batch_workspace_bytes": (ctypes.c_size_t, [_jobp, ctypes.c_int]),
     "zkb_msm_batch": (ctypes.c_int, [_jobp, ctypes.c_int, _vp, ctypes.c_size_t, _vp]),
+    "zkb_msm_table_bytes": (ctypes.c_size_t, [_i64, ctypes.c_int]),
+    "zkb_msm_table_build": (ctypes.c_int, [_u64p, _i64, ctypes.c_int, _u64p, _vp]),
+    "zkb_msm_fixed_batch_workspace_bytes": (ctypes.c_size_t, [_jobp, ctypes.c_int]),
+    "zkb_msm_fixed_batch": (ctypes.c_int, [_jobp, ctypes.c_int, _vp, ctypes.c_size_t, _vp]),
     "zkb_launch_count": (ctypes.c_uint64, []),
     "zkb_tune_set": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int]),
     "zkb_tune_get": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)]),

@@ -151,6 +151,40 @@ def msm_batch(points: Sequence[Any], scalars: Sequence[Any], *,
     return results_to_points(results)
 
 
+def msm_fixed_batch(table: Any, scalars: Sequence[Any]) -> list[Point]:
+    """
+    sum_i s_i P_i for every job j over the first len(scalars[j]) points of a
+    FixedBaseTable (zkb_msm_fixed_batch): one pipeline for all jobs. Same
+    results as msm_batch over the table's points.
+    """
+    torch = _native.require_cuda()
+    scs = [_rows.to_device(s) for s in scalars]
+    for s in scs:
+        if not _rows.shape_ok(s, (LIMBS,)):
+            raise TypeError(f"scalars must be an (n, 4) uint64 array of limbs, got {_rows._describe(s)}")
+        if int(s.shape[0]) > table.n:
+            raise ValueError(f"Length mismatch: {int(s.shape[0])} scalars for a table of {table.n} points.")
+    if not scs:
+        return []
+    results = torch.empty((len(scs), _RESULT_WORDS), dtype=torch.int64, device="cuda")
+    jobs = (_native.ZkbMsmJob * len(scs))()
+    for j, s in enumerate(scs):
+        jobs[j].points = _native.ptr(table.table)
+        jobs[j].scalars = _native.ptr(s)
+        jobs[j].n = int(s.shape[0])
+        jobs[j].result = _native.ptr(results) + 8 * _RESULT_WORDS * j
+        jobs[j].window_size = table.window_size
+    lib = _native.lib()
+    ws_bytes = lib.zkb_msm_fixed_batch_workspace_bytes(jobs, len(scs))
+    err = _native.last_error()
+    if err:
+        raise ValueError(err)
+    ws = _native.workspace(ws_bytes)
+    _native.check(lib.zkb_msm_fixed_batch(jobs, len(scs), _native.ptr(ws), ws_bytes, _native.stream_ptr()),
+                  "zkb_msm_fixed_batch")
+    return results_to_points(results)
+
+
 def results_to_points(results: Any) -> list[Point]:
     """Points of an (m, 16) int64 result block (zkb_msm's 9 words per row)."""
     from zkgpu.msm_gpu import _result_point

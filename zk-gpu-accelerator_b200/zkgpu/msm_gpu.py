@@ -242,3 +242,57 @@ def msm_pippenger_gpu(
     points = BN254_FQ.to_montgomery(plain).reshape(n, 2, LIMBS)
     sc = _rows.upload(_rows.ints_to_limbs(reduced))
     return _launch(points, sc, n, window_size, True)
+
+
+# ------------------------------------------------------------------
+# Fixed-base tables: many MSMs over one resident base set
+# ------------------------------------------------------------------
+
+TABLE_WINDOWS = range(8, 25)
+
+
+class FixedBaseTable:
+    """
+    Per-window multiples of a resident base set, for many MSMs over it or over
+    any prefix of it (a prover's SRS). There is no counterpart in the
+    reference, whose MSM takes its points with every call.
+
+    The table holds, for each point P_i, the rows 2^(w k) P_i and phi(2^(w k) P_i)
+    for the W = ceil(128 / w) windows of a GLV half (2 W x 64 bytes a point). An
+    MSM over it adds every window's digits into one set of 2^(w-1) buckets, so
+    it reduces one window instead of W and needs no doublings at the end; that
+    leaves room for larger windows and so fewer mixed additions. Results equal
+    msm_pippenger_rows over the same points.
+
+    points      : (N, 2, 4) uint64 Montgomery affine rows of points on the curve
+                  (not checked here: msm_pippenger_rows(..., check_points=True)
+                  or curve_gpu's checks validate them), host or device
+    window_size : 8..24 (default 20)
+    """
+
+    def __init__(self, points: Any, window_size: int = 20) -> None:
+        torch = _native.require_cuda()
+        w = operator.index(window_size)
+        if w not in TABLE_WINDOWS:
+            raise ValueError(f"window_size must be in {TABLE_WINDOWS.start}..{TABLE_WINDOWS.stop - 1}, got {w}")
+        pts = _rows.to_device(points)
+        if not _rows.shape_ok(pts, (2, LIMBS)):
+            raise TypeError(f"points must be an (n, 2, 4) uint64 array of affine points, got {_rows._describe(pts)}")
+        self.n = int(pts.shape[0])
+        self.window_size = w
+        lib = _native.lib()
+        nbytes = int(lib.zkb_msm_table_bytes(self.n, w))
+        self.table = torch.empty(max(nbytes // 8, 1), dtype=torch.uint64, device="cuda")
+        if self.n:
+            _native.check(lib.zkb_msm_table_build(_native.ptr(pts), self.n, w, _native.ptr(self.table),
+                                                  _native.stream_ptr()), "zkb_msm_table_build")
+
+    @property
+    def nbytes(self) -> int:
+        return int(self.table.numel()) * 8
+
+    def msm(self, scalars: Any) -> Point:
+        """sum s_i P_i over the first len(scalars) points of the table."""
+        from zkgpu.batch import msm_fixed_batch
+
+        return msm_fixed_batch(self, [scalars])[0]

@@ -203,9 +203,23 @@ class ProofJob:
             raise RuntimeError("the quotient is not a polynomial of degree <= m - 2")
 
 
-def prove_plain(job: ProofJob, workspaces: dict[str, Any] | None = None) -> None:
-    """One job alone, one call per operation (7 zkb_ntt, 1 pointwise, 4 zkb_msm) on the
-    current stream: the one-at-a-time form the batched scheduler is compared with."""
+def msm_table_jobs(table: Any, entries: list[tuple[int, int, int, int]]) -> Any:
+    """zkb_msm_job rows for MSM entries (points, scalars, n, result) whose points are a prefix
+    of the base set that `table` (a FixedBaseTable) was built from: the table takes their place."""
+    jobs = (_native.ZkbMsmJob * max(len(entries), 1))()
+    for j, (_, sc, n, res) in enumerate(entries):
+        if n > table.n:
+            raise ValueError(f"an MSM of {n} points over a table of {table.n}")
+        jobs[j].points, jobs[j].scalars, jobs[j].n, jobs[j].result = _native.ptr(table.table), sc, n, res
+        jobs[j].window_size = table.window_size
+    return jobs
+
+
+def prove_plain(job: ProofJob, workspaces: dict[str, Any] | None = None, table: Any = None) -> None:
+    """One job alone, one call per operation (7 zkb_ntt, 1 pointwise, 4 MSMs) on the
+    current stream: the one-at-a-time form the batched scheduler is compared with. With a
+    FixedBaseTable of the job's base set, each MSM is one zkb_msm_fixed_batch call of one
+    job over it, else one zkb_msm call."""
     lib = _native.lib()
     f = BN254_FR._field()
     s = _native.stream_ptr()
@@ -226,8 +240,15 @@ def prove_plain(job: ProofJob, workspaces: dict[str, Any] | None = None) -> None
                                   ntt_bytes, s), "zkb_ntt")
     job.h_to_plain()
     for k, (pts, sc, n, res) in enumerate(job.msm_entries()):
-        need = lib.zkb_msm_workspace_bytes(n, 0)
         key = f"msm{k}"
+        if table is not None:
+            jobs = msm_table_jobs(table, [(pts, sc, n, res)])
+            need = lib.zkb_msm_fixed_batch_workspace_bytes(jobs, 1)
+            if key not in ws or ws[key].numel() < need:
+                ws[key] = _native.workspace(need)
+            _native.check(lib.zkb_msm_fixed_batch(jobs, 1, _native.ptr(ws[key]), need, s), "zkb_msm_fixed_batch")
+            continue
+        need = lib.zkb_msm_workspace_bytes(n, 0)
         if key not in ws or ws[key].numel() < need:
             ws[key] = _native.workspace(need)
         _native.check(lib.zkb_msm(pts, sc, n, 0, res, _native.ptr(ws[key]), need, s), "zkb_msm")

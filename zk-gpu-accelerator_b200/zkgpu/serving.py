@@ -54,6 +54,7 @@ from zkgpu.prover import (
     STAGE_QUOTIENT,
     ProofJob,
     ProofRequest,
+    msm_table_jobs,
 )
 
 MAX_NTT_PER_LAUNCH = 64
@@ -179,14 +180,17 @@ class Server:
                   the MSM batches and of the ticks' transforms (the block
                   scheduler serves waiting blocks of higher-priority streams
                   first)
+    table       : optional FixedBaseTable built from `bases`: the MSM batches then
+                  run over it (zkb_msm_fixed_batch), with the same results
     """
 
     def __init__(self, bases: Any, hbm_budget: int, max_ticks_ahead: int = 2, msm_streams: int = 2,
                  msm_priority: str = "high", tick_priority: str = "normal",
-                 max_batch_points: int = 1 << 22) -> None:
+                 max_batch_points: int = 1 << 22, table: Any = None) -> None:
         torch = _native.require_cuda()
         self.torch = torch
         self.bases = bases
+        self.table = table
         self.sched = Scheduler(hbm_budget)
         self.max_ticks_ahead = max_ticks_ahead
         lo, hi = torch.cuda.Stream.priority_range()
@@ -220,7 +224,9 @@ class Server:
         jobs = (_native.ZkbMsmJob * 4)()
         for k, n in enumerate((m, m, m - 2, m - 1)):
             jobs[k].points, jobs[k].scalars, jobs[k].n, jobs[k].result = 256, 256, n, 256
-        msm_ws = int(lib.zkb_msm_batch_workspace_bytes(jobs, 4))
+            jobs[k].window_size = self.table.window_size if self.table is not None else 0
+        msm_ws = int(lib.zkb_msm_fixed_batch_workspace_bytes(jobs, 4) if self.table is not None
+                     else lib.zkb_msm_batch_workspace_bytes(jobs, 4))
         return buffers + ntt_ws + msm_ws
 
     # ---- the loop -----------------------------------------------------------
@@ -316,17 +322,22 @@ class Server:
             work, self.pending_msm = self.pending_msm[:take], self.pending_msm[take:]
             entries = [e for w in work for e in w[0]]
             ids = [j for w in work for j in w[1]]
-            jobs = (_native.ZkbMsmJob * len(entries))()
-            for j, (pts, sc, n, res) in enumerate(entries):
-                jobs[j].points, jobs[j].scalars, jobs[j].n, jobs[j].result = pts, sc, n, res
+            if self.table is not None:
+                jobs = msm_table_jobs(self.table, entries)
+                size_fn, run_fn, name = lib.zkb_msm_fixed_batch_workspace_bytes, lib.zkb_msm_fixed_batch, \
+                    "zkb_msm_fixed_batch"
+            else:
+                jobs = (_native.ZkbMsmJob * len(entries))()
+                for j, (pts, sc, n, res) in enumerate(entries):
+                    jobs[j].points, jobs[j].scalars, jobs[j].n, jobs[j].result = pts, sc, n, res
+                size_fn, run_fn, name = lib.zkb_msm_batch_workspace_bytes, lib.zkb_msm_batch, "zkb_msm_batch"
             for w in work:
                 stream.wait_event(w[2])  # the witness / h these MSMs read is written
             before = int(lib.zkb_launch_count())
             with torch.cuda.stream(stream):
-                ws_bytes = int(lib.zkb_msm_batch_workspace_bytes(jobs, len(entries)))
+                ws_bytes = int(size_fn(jobs, len(entries)))
                 ws = _native.workspace(ws_bytes)
-                _native.check(lib.zkb_msm_batch(jobs, len(entries), _native.ptr(ws), ws_bytes,
-                                                _native.stream_ptr()), "zkb_msm_batch")
+                _native.check(run_fn(jobs, len(entries), _native.ptr(ws), ws_bytes, _native.stream_ptr()), name)
                 done = torch.cuda.Event(enable_timing=True)
                 done.record(stream)
             self.launches += int(lib.zkb_launch_count()) - before
