@@ -347,3 +347,44 @@ def test_per_size_tables_drive_the_plans(tmp_path):
         autotune.clear()
     assert lib.zkb_msm_default_window(3000) == model
     assert lib.zkb_ntt_workspace_bytes(512) == 0
+
+
+# ------------------------------------------------------------------
+# Fixed-base tables: host-side checks (no GPU needed)
+# ------------------------------------------------------------------
+
+
+def test_fixed_base_table_window_is_checked_first():
+    from zkgpu.msm_gpu import FixedBaseTable
+
+    for w in (7, 25, 0):
+        with pytest.raises(ValueError, match="window_size must be in 8..24"):
+            FixedBaseTable(np.zeros((4, 2, 4), dtype=np.uint64), w)
+    with pytest.raises(TypeError):
+        FixedBaseTable(np.zeros((4, 2, 4), dtype=np.uint64), 16.0)
+
+
+def test_table_job_rows_and_their_limit():
+    """msm_table_jobs puts the table in place of the base set's prefix, with its window."""
+    import types
+
+    import torch
+
+    from zkgpu.prover import msm_table_jobs
+
+    table = types.SimpleNamespace(n=100, window_size=16, table=torch.zeros(8, dtype=torch.uint64))
+    jobs = msm_table_jobs(table, [(111, 222, 100, 333), (111, 444, 5, 555)])
+    assert [(j.points, j.scalars, j.n, j.result, j.window_size) for j in jobs] == [
+        (table.table.data_ptr(), 222, 100, 333, 16), (table.table.data_ptr(), 444, 5, 555, 16)]
+    with pytest.raises(ValueError, match="101 points over a table of 100"):
+        msm_table_jobs(table, [(111, 222, 101, 333)])
+
+
+def test_table_sizes_follow_the_window():
+    from zkgpu import _native
+
+    lib = _native.lib()
+    assert lib.zkb_msm_table_bytes(1 << 20, 16) == (1 << 20) * 16 * 64
+    assert lib.zkb_msm_table_bytes(1000, 22) == 1000 * 12 * 64
+    assert lib.zkb_msm_table_bytes(1000, 7) == 0 and lib.zkb_msm_table_bytes(1000, 25) == 0
+    assert lib.zkb_msm_table_bytes(0, 16) == 0

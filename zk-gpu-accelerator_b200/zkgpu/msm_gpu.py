@@ -271,10 +271,10 @@ class FixedBaseTable:
     """
 
     def __init__(self, points: Any, window_size: int = 20) -> None:
-        torch = _native.require_cuda()
         w = operator.index(window_size)
         if w not in TABLE_WINDOWS:
             raise ValueError(f"window_size must be in {TABLE_WINDOWS.start}..{TABLE_WINDOWS.stop - 1}, got {w}")
+        torch = _native.require_cuda()
         pts = _rows.to_device(points)
         if not _rows.shape_ok(pts, (2, LIMBS)):
             raise TypeError(f"points must be an (n, 2, 4) uint64 array of affine points, got {_rows._describe(pts)}")
