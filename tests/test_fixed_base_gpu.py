@@ -120,3 +120,22 @@ def test_served_jobs_over_a_table_equal_the_jobs_alone():
     assert len(recs) == len(reqs)
     for job_id, job in keep.items():
         assert job.msm_points() == alone[job_id], job_id
+
+
+def test_full_batches_of_64_jobs():
+    """The largest batch (64 jobs) through the counting-sort pipeline and over a table: sizes
+    from 0 to 2^11, uniform and skewed scalars, against one MSM per job."""
+    import torch
+
+    bases = _bases(1 << 11, 9)
+    table = FixedBaseTable(bases, 10)
+    rng = np.random.default_rng(3)
+    sizes = [0, 1] + [int(v) for v in rng.integers(2, 1 << 11, size=62)]
+    scs = []
+    for k, n in enumerate(sizes):
+        gen = wl.uniform_fr if k % 2 else wl.skewed_scalars
+        scs.append(torch.from_numpy(gen(500 + k, n) if n else np.zeros((0, 4), dtype=np.uint64)).cuda())
+    one_by_one = [msm_gpu.msm_pippenger_rows(bases[:n], s, check_points=False) if n else Point.identity()
+                  for n, s in zip(sizes, scs, strict=True)]
+    assert batch.msm_batch([bases[:n] for n in sizes], scs) == one_by_one
+    assert batch.msm_fixed_batch(table, scs) == one_by_one
