@@ -773,9 +773,13 @@ def run_int64(log_n: int = 25, log_ops: int = 26, cpu: bool = True) -> dict:
     ntt_gbs = 16 * n / t_ntt / 1e6
     mul_gbs = 24 * m / t_mul / 1e6
     passes = 1 + -(-(log_n - 10) // 10)
+    # a modulus below 2^31 (998244353 = 119 2^23 + 1, its largest size): the 32-bit butterflies
+    small = torch.randint(0, 998_244_353, (1 << 23,), device="cuda", generator=g)
+    t_small = _event_ms(lambda: ntt_gpu(small, 998_244_353), 10)
     out = {
         "workload": f"forward NTT of 2^{log_n} int64 words mod {INT64_NTT_PRIME} (k 2^32 + 1); "
                     f"element-wise product of 2^{log_ops} words",
+        "ntt_998244353_2e23_ms": round(t_small, 4),
         "ntt_ms": round(t_ntt, 4),
         "ntt_passes": passes,
         "ntt_roofline": {"bound": "hbm", "achieved": round(ntt_gbs, 1), "peak": hbm, "unit": "GB/s",

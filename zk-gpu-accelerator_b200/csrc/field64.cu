@@ -111,7 +111,8 @@ __global__ void __launch_bounds__(256) k_u64_pow(const int64_t* bases, int64_t* 
 // ---- NTT over a prime m < 2^63 ---------------------------------------------
 //
 // Radix-2 DIT on bit-reversed input (the order of zkgpu/ntt.py:149-203), in
-// two to four passes over HBM instead of one per stage. The data stays in
+// two to four passes over HBM instead of one per stage; 32-bit butterflies for
+// moduli below 2^31. The data stays in
 // plain form and every twiddle w carries its Shoup quotient w' = floor(w 2^64 / m),
 // so b w mod m = b w - umulhi(b, w') m (mod 2^64), less m at most once: about
 // two thirds of a Montgomery product. w' comes without a division: from
@@ -156,18 +157,41 @@ __device__ __forceinline__ Tw64 tw64_from_mont(uint64_t wm, const Mod64& M) {
   return Tw64{mont64(wm, 1, M), wm * M.ninv};
 }
 
+// Moduli below 2^31 (most NTT-friendly primes: 998244353, 7340033, 12289) take
+// the same butterflies in 32-bit words (k32): Shoup's product with the quotient
+// floor(w 2^32 / m), which is the stored floor(w 2^64 / m) shifted down by 32.
+// b w mod m for b < 2^32 and w < m < 2^31.
+__device__ __forceinline__ uint32_t shoup32(uint32_t b, uint32_t w, uint32_t q, uint32_t m) {
+  const uint32_t r = b * w - __umulhi(b, q) * m;  // in [0, 2m)
+  return r >= m ? r - m : r;
+}
+
+template <bool k32>
+__device__ __forceinline__ uint64_t mulw64(uint64_t b, Tw64 t, uint64_t m) {
+  if (k32) return shoup32((uint32_t)b, (uint32_t)t.w, (uint32_t)(t.q >> 32), (uint32_t)m);
+  return shoup64(b, t, m);
+}
+
 // (a, b) <- (a + b w, a - b w)
+template <bool k32>
 __device__ __forceinline__ void bfly64(uint64_t& a, uint64_t& b, Tw64 w, uint64_t m) {
-  const uint64_t v = shoup64(b, w, m), u = a;
+  const uint64_t v = mulw64<k32>(b, w, m), u = a;
+  if (k32) {
+    const uint32_t x = (uint32_t)u, y = (uint32_t)v, mm = (uint32_t)m, sum = x + y;  // < 2^32
+    a = sum >= mm ? sum - mm : sum;
+    b = x >= y ? x - y : x + (mm - y);
+    return;
+  }
   a = addmod64(u, v, m);
   b = submod64(u, v, m);
 }
 
 // the same with the twiddle given as two factors: (a, b) <- (a + b w1 w2, a - b w1 w2)
+template <bool k32>
 __device__ __forceinline__ void bfly64(uint64_t& a, uint64_t& b, Tw64 w1, Tw64 w2, uint64_t m) {
-  const uint64_t v = shoup64(shoup64(b, w1, m), w2, m), u = a;
-  a = addmod64(u, v, m);
-  b = submod64(u, v, m);
+  uint64_t t = mulw64<k32>(b, w1, m);
+  bfly64<k32>(a, t, w2, m);
+  b = t;
 }
 
 // omega^e R from the powers omega^(2^k) R (one product per set bit of e)
@@ -193,7 +217,7 @@ __global__ void __launch_bounds__(256) k_ntt64_stage_table(Tw64* tst, int count,
   }
 }
 
-template <bool kFirst>
+template <bool kFirst, bool k32>
 __global__ void __launch_bounds__(kNtt64Threads) k_ntt64_pass(const int64_t* in, int64_t* out, int log_n, int S,
                                                               int K, int c, const Tw64* tst, Ntt64Roots P,
                                                               uint64_t one, Tw64 scale, int scaled, Mod64 M) {
@@ -277,22 +301,22 @@ __global__ void __launch_bounds__(kNtt64Threads) k_ntt64_pass(const int64_t* in,
       uint64_t x0 = s[i0], x1 = s[i0 + d], x2 = s[i0 + 2 * d], x3 = s[i0 + 3 * d];
       if (kFirst) {
         const Tw64 w0 = tw[h + rlo], w1 = tw[2 * h + rlo], w2 = tw[3 * h + rlo];
-        bfly64(x0, x1, w0, m);
-        bfly64(x2, x3, w0, m);
-        bfly64(x0, x2, w1, m);
-        bfly64(x1, x3, w2, m);
+        bfly64<k32>(x0, x1, w0, m);
+        bfly64<k32>(x2, x3, w0, m);
+        bfly64<k32>(x0, x2, w1, m);
+        bfly64<k32>(x1, x3, w2, m);
       } else if (invariant) {
-        bfly64(x0, x1, f0, m);
-        bfly64(x2, x3, f0, m);
-        bfly64(x0, x2, f1, m);
-        bfly64(x1, x3, f2, m);
+        bfly64<k32>(x0, x1, f0, m);
+        bfly64<k32>(x2, x3, f0, m);
+        bfly64<k32>(x0, x2, f1, m);
+        bfly64<k32>(x1, x3, f2, m);
       } else {
         const Tw64 w0 = tw[h + rlo], w1 = tw[2 * h + rlo], w2 = tw[3 * h + rlo];
         const Tw64 b0 = base[t * C + col], b1 = base[(t + 1) * C + col];
-        bfly64(x0, x1, w0, b0, m);
-        bfly64(x2, x3, w0, b0, m);
-        bfly64(x0, x2, w1, b1, m);
-        bfly64(x1, x3, w2, b1, m);
+        bfly64<k32>(x0, x1, w0, b0, m);
+        bfly64<k32>(x2, x3, w0, b0, m);
+        bfly64<k32>(x0, x2, w1, b1, m);
+        bfly64<k32>(x1, x3, w2, b1, m);
       }
       s[i0] = x0;
       s[i0 + d] = x1;
@@ -309,9 +333,9 @@ __global__ void __launch_bounds__(kNtt64Threads) k_ntt64_pass(const int64_t* in,
       const int i0 = ((((q >> t) << (t + 1)) | rlo) << c) | col;
       uint64_t x0 = s[i0], x1 = s[i0 + d];
       if (kFirst) {
-        bfly64(x0, x1, tw[h + rlo], m);
+        bfly64<k32>(x0, x1, tw[h + rlo], m);
       } else {
-        bfly64(x0, x1, tw[h + rlo], base[t * C + col], m);
+        bfly64<k32>(x0, x1, tw[h + rlo], base[t * C + col], m);
       }
       s[i0] = x0;
       s[i0 + d] = x1;
@@ -321,7 +345,7 @@ __global__ void __launch_bounds__(kNtt64Threads) k_ntt64_pass(const int64_t* in,
   for (int e = threadIdx.x; e < E; e += blockDim.x) {
     const int64_t col = e & (C - 1), row = e >> c;
     const int64_t r = kFirst ? fixed + row + (col << (log_n - c)) : fixed + col + (row << S);
-    out[r] = (int64_t)(scaled ? shoup64(s[e], scale, m) : s[e]);
+    out[r] = (int64_t)(scaled ? mulw64<k32>(s[e], scale, m) : s[e]);
   }
 }
 
@@ -482,7 +506,9 @@ int zkb_ntt64(const int64_t* in, int64_t* out, int64_t n, int64_t mod, int64_t o
     const size_t smem = ((size_t)8 << (p.K + p.c)) + ((size_t)sizeof(Tw64) << p.K) +
                         (i == 0 ? 0 : (size_t)(p.K << p.c) * (sizeof(Tw64) + 8));
     const int scaled = invert && i == count - 1;
-    auto kern = i == 0 ? k_ntt64_pass<true> : k_ntt64_pass<false>;
+    const bool k32 = m < (1ull << 31);
+    auto kern = i == 0 ? (k32 ? k_ntt64_pass<true, true> : k_ntt64_pass<true, false>)
+                       : (k32 ? k_ntt64_pass<false, true> : k_ntt64_pass<false, false>);
     ZKB_TRY(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                        "int64 NTT shared memory attribute"));
     ProfSpan span(i == 0 ? "ntt64_first_pass" : "ntt64_later_pass", s);
