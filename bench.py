@@ -486,6 +486,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
                    "schedule": "one MSM batch (both MSMs, one pipeline) + one persistent NTT launch (both "
                                "transforms) on a side stream beside it"},
         "parts_ms": {k: round(v, 3) for k, v in part_ms.items()},
+        "msm_points_per_s": {k: round(step.n / (v * 1e-3)) for k, v in part_ms.items() if k.startswith("msm")},
         "sequential_ms": round(sum(part_ms.values()), 3),
         "same_as_one_call_results": same,
         "stages_ms": {k: round(v[1] / v[0], 4) for k, v in {**prof_msm, **prof_ntt}.items()},
