@@ -3,7 +3,7 @@ bench.py — the BN254 prover hot path on B200: large plain instances.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload large|small]
 
-Workload "large" (default; BASELINE.json's metric is quoted on it): one step =
+Workload "large" (default; the headline metric is quoted on it): one step =
   MSM over 2^22 BN254 G1 points with uniform scalars
   + the same MSM with skewed witness-like scalars (60% in {0,1}, 20% < 2^32)
   + a forward Fr NTT of 2^24 elements

@@ -3,7 +3,7 @@ The oracle, pinned: both restatements (oracle.pyoracle, oracle.c_oracle)
 against golden vectors produced by running the reference itself
 (tests/golden/make_golden.py) and against the known answers in the
 reference's own tests. CPU only; these make the oracle trustworthy before it
-judges the GPU.
+checks the GPU's results.
 """
 
 from __future__ import annotations
