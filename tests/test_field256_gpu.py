@@ -107,6 +107,45 @@ def test_squaring_matches_python(field):
     assert F.to_ints(F.mul(one, one)) == [1]
 
 
+def extreme_values(p: int, seed: int) -> list[int]:
+    """Canonical values whose 32-bit words push the product's carry chains to their ends: p - 1 and
+    its neighbours, words of all ones, p minus powers of 2^32, and values whose words are each 0,
+    0xffffffff or random (the top bits cleared to stay below p, so the word pattern survives)."""
+    vals = {0, 1, 2, p - 1, p - 2, p - 3}
+    for k in range(1, 9):
+        vals.add(min(p - 1, (1 << (32 * k)) - 1))
+        vals.add(p - (1 << (32 * (k - 1))))
+        vals.add(p - 1 - ((1 << (32 * (k - 1))) - 1))
+    rng = random.Random(seed)
+    keep = (1 << (p.bit_length() - 1)) - 1
+    while len(vals) < 72:
+        v = 0
+        for w in range(8):
+            v |= rng.choice((0, 0xFFFFFFFF, 0xFFFFFFFF, rng.getrandbits(32))) << (32 * w)
+        vals.add(v if v < p else v & keep)
+    return sorted(vals)
+
+
+@pytest.mark.parametrize("field", FIELDS[:3])
+def test_raw_rows_with_extreme_words(field):
+    """The Montgomery product and squaring on raw rows (no conversion, so the kernel sees these exact
+    words): every pair of the extreme values gives a b 2^-256 mod p, every square a^2 2^-256 mod p."""
+    from zkgpu import _rows
+
+    p = field.modulus
+    vals = extreme_values(p, p % 1009)
+    a = [x for x in vals for _ in vals]
+    b = vals * len(vals)
+    rinv = pow(2**256, -1, p)
+    A = _rows.upload(_rows.ints_to_limbs(a))
+    B = _rows.upload(_rows.ints_to_limbs(b))
+    got = _rows.limbs_to_ints(_rows.download(field.mul(A, B)))
+    assert got == [x * y * rinv % p for x, y in zip(a, b, strict=True)]
+    S = _rows.upload(_rows.ints_to_limbs(vals))
+    got = _rows.limbs_to_ints(_rows.download(field.mul(S, S)))  # the same rows: the squaring path
+    assert got == [x * x * rinv % p for x in vals]
+
+
 def test_operations_compose():
     F, p = BN254_FQ, P
     a, b = operands(p, 4)
