@@ -111,7 +111,7 @@ __global__ void __launch_bounds__(256) k_u64_pow(const int64_t* bases, int64_t* 
 // ---- NTT over a prime m < 2^63 ---------------------------------------------
 //
 // Radix-2 DIT on bit-reversed input (the order of zkgpu/ntt.py:149-203), in
-// two to four passes over HBM instead of one per stage; 32-bit butterflies for
+// one to four passes over HBM instead of one per stage; 32-bit butterflies for
 // moduli below 2^31. The data stays in
 // plain form and every twiddle w carries its Shoup quotient w' = floor(w 2^64 / m),
 // so b w mod m = b w - umulhi(b, w') m (mod 2^64), less m at most once: about
@@ -355,18 +355,30 @@ struct Ntt64Pass {
 
 // first pass: stages 0 .. K1-1 on tiles of 2^c1 columns (none below 2^(2 c1)); the
 // rest split evenly into passes of at most kL stages on 2^c-column tiles. Shapes by
-// size, measured on B200 (ms for the forward transform, by (c1, K1, c, kL)):
-// 2^20: (5, 8, 5, 8) 0.070, (3, 9, 4, 8) 0.087, (2, 10, 3, 9) 0.143;
-// 2^22: (5, 8, 5, 8) 0.184, (3, 9, 4, 8) 0.218, (2, 10, 3, 9) 0.359;
-// 2^25: (3, 9, 4, 8) 1.26, (5, 8, 5, 8) 2.27, (2, 10, 3, 9) 1.74.
+// size, measured on B200 (ms for the forward transform by (c1, K1, c, kL), over a
+// 63-bit modulus / over 998244353, whose butterflies are 32-bit; every shape of
+// {5 8, 4 9, 3 10} x {5 8, 4 9, 3 10} timed, the best and the runner-up given):
+// 2^16: (3, 10, 3, 10) 0.036 / 0.030, (5, 8, 5, 8) 0.051 / 0.039;
+// 2^20: (3, 10, 3, 10) 0.056 / 0.040, (5, 8, 5, 8) 0.069 / 0.052;
+// 2^22: (5, 8, 5, 8) 0.183 / 0.124, (4, 9, 5, 8) 0.188 / 0.128;
+// 2^23: (5, 8, 5, 8) 0.337 / 0.215, (3, 9, 4, 8) 0.378 / 0.264;
+// 2^24: (4, 9, 5, 8) 0.655, (3, 9, 4, 8) 0.688;
+// 2^25: (3, 9, 4, 8) 1.26, (3, 10, 5, 8) 1.29, (5, 8, 5, 8) 2.27.
 static int plan_ntt64(int log_n, Ntt64Pass* passes) {
-  const bool large = log_n > 22;
+  int dcf = 3, dkf = 9, dcl = 4, dkl = 8;  // from 2^25
+  if (log_n <= 20) {
+    dcf = 3, dkf = 10, dcl = 3, dkl = 10;
+  } else if (log_n <= 23) {
+    dcf = 5, dkf = 8, dcl = 5, dkl = 8;
+  } else if (log_n == 24) {
+    dcf = 4, dkf = 9, dcl = 5, dkl = 8;
+  }
   int cf = (int)tune_get("ntt64.first_col_log"), kf = (int)tune_get("ntt64.first_max_k");
   int cl = (int)tune_get("ntt64.col_log"), kL = (int)tune_get("ntt64.max_k");
-  if (cf < 0) cf = large ? 3 : 5;
-  if (kf < 4) kf = large ? 9 : 8;
-  if (cl < 1) cl = large ? 4 : 5;
-  if (kL < 2) kL = 8;
+  if (cf < 0) cf = dcf;
+  if (kf < 4) kf = dkf;
+  if (cl < 1) cl = dcl;
+  if (kL < 2) kL = dkl;
   const int c1 = log_n >= 2 * cf ? cf : 0;
   int K1 = log_n - c1 < kf ? log_n - c1 : kf;
   if (K1 + c1 > kNtt64MaxTileLog) K1 = kNtt64MaxTileLog - c1;
