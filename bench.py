@@ -96,11 +96,11 @@ _GLV_G2 = 0x24CCEF014A773D2CF7A7BD9D4391EB18E
 
 def ntt_products(n: int, log_n: int) -> int:
     """Montgomery products of one forward NTT of n = 2^log_n rows as csrc/ntt.cu runs it: log_n
-    split into P passes (at most 12 bits each, two from 2^10); a pass of 2^lr rows does lr / 2
-    radix-4 rounds, the first with only the w_4 product (1 per 4 rows), the others 4 per 4 rows,
-    plus a radix-2 stage (1 per 2 rows) for odd lr; each pass boundary 1 product per row (the
-    twiddle read from the expanded table)."""
-    P = max(-(-log_n // 12), 2 if log_n >= 10 else 1)
+    split into P passes (three from 2^19, else at most 12 bits each and two from 2^10); a pass of
+    2^lr rows does lr / 2 radix-4 rounds, the first with only the w_4 product (1 per 4 rows), the
+    others 4 per 4 rows, plus a radix-2 stage (1 per 2 rows) for odd lr; each pass boundary 1
+    product per row (the twiddle read from the expanded table)."""
+    P = 3 if log_n >= 19 else max(-(-log_n // 12), 2 if log_n >= 10 else 1)
     radices = [log_n // P + (1 if q < log_n % P else 0) for q in range(P)]
     per_row = 0.0
     for lr in radices:
@@ -335,6 +335,9 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     device = torch.device("cuda", local_rank)
     dist = init_dist(world, "nccl")
     log_msm, log_ntt = WORKLOADS[args.workload]
+    for kv in args.knob:  # library tuning knobs, before anything plans its work
+        key, _, value = kv.partition("=")
+        _native.tune_set(key.strip(), int(value))
     tuned = None
     if args.tune:
         from zkgpu import autotune
@@ -483,8 +486,9 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
                    "scalars": ["uniform [0,r)", "skewed 60% {0,1} / 20% < 2^32 / 20% uniform"],
                    "l2": "every input larger than the 126 MB L2 (bases 256 MiB, NTT 512 MiB)",
                    "parallelism": f"replicas x{world}",
-                   "schedule": "one MSM batch (both MSMs, one pipeline) + one persistent NTT launch (both "
-                               "transforms) on a side stream beside it"},
+                   "schedule": "one MSM batch (both MSMs, one pipeline) on a high-priority stream; both "
+                               "transforms as pass launches (zkb_ntt each) on a low-priority stream beside it",
+                   **({"knobs": dict(kv.split("=", 1) for kv in args.knob)} if args.knob else {})},
         "parts_ms": {k: round(v, 3) for k, v in part_ms.items()},
         "msm_points_per_s": {k: round(step.n / (v * 1e-3)) for k, v in part_ms.items() if k.startswith("msm")},
         "sequential_ms": round(sum(part_ms.values()), 3),
@@ -1018,6 +1022,8 @@ def main() -> None:
     ap.add_argument("--skip-batched", action="store_true", help="skip the batched form (64 NTTs + 32 MSMs)")
     ap.add_argument("--skip-served", action="store_true", help="skip the served form (Poisson job stream)")
     ap.add_argument("--skip-int64", action="store_true", help="skip the int64 field / NTT figures")
+    ap.add_argument("--knob", action="append", default=[], metavar="KEY=VALUE",
+                    help="set a library tuning knob (zkb_tune_set) before the run; repeatable")
     ap.add_argument("--tune", action="store_true",
                     help="measure (or load from the cache) per-size MSM windows and NTT shapes first")
     args = ap.parse_args()

@@ -327,11 +327,12 @@ int zkb_msm_fixed_batch(const zkb_msm_job* jobs, int count, void* workspace, siz
  * "msm.slots_per_thread" (8), "msm.reduce_log_segment" (2), "msm.sort" (1:
  * pairs grouped by a counting sort that skips zero digits; 0: a radix sort
  * of all pairs; the same points either way),
- * "ntt.max_log_radix" (12, range 8..12: the largest sub-transform one NTT pass
- * does), "ntt.cta_log_elems" (log2 of the rows staged per NTT block, 9..12;
- * default 0 = 12 for large transforms, 10 when fewer than four 4096-row
- * blocks per SM), "ntt.threads" (threads per NTT block, 64..512; default 0 =
- * 512 for 4096-row blocks, else 256); the int64 NTT's tile shapes
+ * "ntt.max_log_radix" (log2 of the largest sub-transform one NTT pass does,
+ * 8..12; default 0 = by size: three passes from 2^19 rows, else up to 12),
+ * "ntt.cta_log_elems" (log2 of the rows staged per NTT block, 9..12; default
+ * 0 = 9: a block holds one sub-transform once those reach 512 rows),
+ * "ntt.threads" (threads per NTT block, 64..512; default 0 = by the block's
+ * rows: 128 up to 512, 256 up to 2048, 512 for 4096); the int64 NTT's tile shapes
  * "ntt64.first_col_log" (input words per row of a first-pass tile, log2, 0..6;
  * -1 = by size), "ntt64.first_max_k" (first-pass stages, 4..10; 0 = by size),
  * "ntt64.col_log" (words per row of a later-pass tile, log2, 1..6; 0 = by size),

@@ -67,7 +67,7 @@ def test_ntt_batch_with_three_pass_transforms():
         for x, y, i, c in zip(xs, outs, [False, True, False, True, False], [5, None, 7, 5, None], strict=True):
             assert bool((y == BN254_FR.ntt(x, invert=i, coset=c)).all()), int(x.shape[0])
     finally:
-        _native.tune_set("ntt.max_log_radix", 12)
+        _native.tune_set("ntt.max_log_radix", 0)
 
 
 def test_ntt_batch_round_trip_and_limits():

@@ -257,6 +257,8 @@ def test_ntt_matches_c_oracle_between_fixture_sizes(log_n):
     "knobs",
     [
         {"ntt.max_log_radix": 8},  # three passes at 2^20 and above
+        {"ntt.max_log_radix": 12},  # two passes up to 2^24 (4096-row tiles of 512 threads there)
+        {"ntt.max_log_radix": 12, "ntt.cta_log_elems": 10},  # 1024-row tiles of 256 threads
         {"ntt.max_log_radix": 9, "ntt.cta_log_elems": 9, "ntt.threads": 64},
         {"ntt.cta_log_elems": 12, "ntt.threads": 128},
         {"ntt.cta_log_elems": 10, "ntt.threads": 512},
@@ -291,7 +293,7 @@ def test_ntt_pass_plans_give_the_same_rows(knobs):
                 got = BN254_FR.ntt(rows, invert=invert, coset=coset).cpu().numpy()
                 assert np.array_equal(got, want), (log_n, invert, coset)
     finally:
-        _native.tune_set("ntt.max_log_radix", 12)
+        _native.tune_set("ntt.max_log_radix", 0)
         _native.tune_set("ntt.cta_log_elems", 0)
         _native.tune_set("ntt.threads", 0)
         _native.tune_set("ntt.full_table_mb", 4096)

@@ -94,12 +94,12 @@ def test_host_only_queries():
 
 def test_tuning_knobs_validate_and_plan_the_workspace():
     defaults = {"msm.pairs_per_thread": 64, "msm.slots_per_thread": 8, "msm.reduce_log_segment": 2, "msm.sort": 1,
-                "ntt.max_log_radix": 12, "ntt.cta_log_elems": 0, "ntt.threads": 0, "ntt.full_table_mb": 4096,
+                "ntt.max_log_radix": 0, "ntt.cta_log_elems": 0, "ntt.threads": 0, "ntt.full_table_mb": 4096,
                 "ntt64.first_col_log": -1, "ntt64.first_max_k": 0, "ntt64.col_log": 0, "ntt64.max_k": 0}
     assert {k: _native.tune_get(k) for k in defaults} == defaults
     with pytest.raises(ValueError, match="unknown tuning knob"):
         _native.tune_set("ntt.bogus", 1)
-    with pytest.raises(ValueError, match="8..12"):
+    with pytest.raises(ValueError, match="0..12"):
         _native.tune_set("ntt.max_log_radix", 13)
     lib = _native.lib()
     try:
@@ -109,7 +109,7 @@ def test_tuning_knobs_validate_and_plan_the_workspace():
         assert lib.zkb_ntt_workspace_bytes(512) == 512 * 32
         assert lib.zkb_ntt_workspace_bytes(256) == 0
     finally:
-        _native.tune_set("ntt.max_log_radix", 12)
+        _native.tune_set("ntt.max_log_radix", 0)
     assert lib.zkb_ntt_workspace_bytes(512) == 0
 
 

@@ -627,9 +627,20 @@ static int ilog2(int64_t n) {
 // 2^5..2^6-point sub-transforms spread it over 32-64 CTAs (2^12 rows: 0.048
 // ms instead of 0.11 ms on a B200).
 // A per-size table entry (an autotuner's) takes precedence over the knob.
-static std::vector<int> plan_radices(int log_n) {
+// The radices (log2 sub-transform sizes) of the passes of a 2^log_n-row NTT.
+// The largest sub-transform per pass comes from a per-size table entry, else the
+// "ntt.max_log_radix" knob, else the size. A single transform takes three passes
+// from 2^19 rows (256-row sub-transforms at 2^24), else up to 4096 rows a pass:
+// measured on B200 with 512-row tiles of 128 threads, 2^24 rows 4.96 ms in three
+// passes against 5.74 in two 4096-row passes, 2^23 2.41 against 2.94, 2^20 0.300
+// against 0.306; two passes stay best to 2^18 (0.0929 against 0.0946). A batch
+// (`batch`) keeps up to 4096 rows a pass: its persistent kernel starts a pass's
+// tiles only after the transform's previous pass, and the served jobs' small
+// batches measured far slower with the third pass.
+static std::vector<int> plan_radices(int log_n, bool batch = false) {
   const int tuned = tune_get_sized("ntt.max_log_radix", log_n);
-  const int max_r = tuned > 0 ? tuned : tune_get("ntt.max_log_radix");
+  int max_r = tuned > 0 ? tuned : tune_get("ntt.max_log_radix");
+  if (max_r < 8) max_r = log_n >= 19 && !batch ? (log_n + 2) / 3 : kMaxLogR;
   int P = (log_n + max_r - 1) / max_r;
   if (P > 3) P = 3;
   if (P < (log_n + kMaxLogR - 1) / kMaxLogR) P = (log_n + kMaxLogR - 1) / kMaxLogR;
@@ -844,28 +855,31 @@ struct PassLaunch {
 
 // The passes of one transform. cta_log / threads: the tile and block size,
 // or 0 for the size-based choice (and the "ntt.cta_log_elems" / "ntt.threads"
-// knobs, which override it).
+// knobs, which override it). batch: the transform is part of a batch launch
+// (the pass split of plan_radices for batches).
 static void plan_passes(int64_t n, int log_n, int invert, const RootTables& rt,
                         const ScaleTables& st, const uint64_t* in, uint64_t* out, uint64_t* tmp,
-                        int sms, int cta_log, int threads, std::vector<PassLaunch>& passes) {
-  const std::vector<int> radices = plan_radices(log_n);
+                        int cta_log, int threads, bool batch, std::vector<PassLaunch>& passes) {
+  const std::vector<int> radices = plan_radices(log_n, batch);
   const int P = (int)radices.size();
-  // columns per CTA: the tile C R is at most 2^cta_log elements. Auto:
-  // 4096-row tiles of 512 threads (one CTA per SM, 128 KiB of shared memory)
-  // when that gives at least 16 CTAs per SM (2^24 rows and up on a B200),
-  // else 1024-row tiles of 256 threads, several per SM, which measured faster
-  // from 2^12 to 2^22 rows.
+  // columns per CTA: the tile C R is at most 2^cta_log elements, and at least
+  // one sub-transform. Auto: 512-row tiles (one column once a pass's
+  // sub-transform has 512 rows), with 128 threads up to 512-row tiles, 256 up
+  // to 2048 and 512 for 4096. Small tiles put several CTAs on each SM, so one
+  // CTA's loads and barriers overlap another's products; measured on B200
+  // against 1024-row tiles of 256 threads (and 4096-row tiles of 512 threads
+  // from 2^24): 18-27 % faster from 2^11 to 2^16 rows, within 2 % at 2^17-2^18.
   // A per-size table entry takes precedence over the knob, which takes
   // precedence over the rule.
   if (cta_log == 0) {
     cta_log = tune_get_sized("ntt.cta_log_elems", log_n);
     if (cta_log < 9) cta_log = tune_get("ntt.cta_log_elems");
-    if (cta_log < 9) cta_log = (n >> kMaxLogR) >= 16 * sms ? kMaxLogR : 10;
+    if (cta_log < 9) cta_log = 9;
   }
   if (threads == 0) {
     threads = tune_get_sized("ntt.threads", log_n);
     if (threads < 64) threads = tune_get("ntt.threads");
-    if (threads < 64) threads = cta_log >= kMaxLogR ? 512 : 256;
+    if (threads < 64) threads = 0;  // by each pass's tile, below
   }
   passes.clear();
   int ls = log_n;  // stride exponent of the current pass: S_q = 2^(log_n - sum of radices so far)
@@ -908,7 +922,8 @@ static void plan_passes(int64_t n, int log_n, int invert, const RootTables& rt,
     // padded columns, then the stage table (R / 2 rows)
     L.smem = (size_t)(1 << lc) * ((32u << a.lr) + 16) + ((size_t)16 << a.lr);
     const int half_total = (1 << (a.lr + lc)) >> 1;
-    L.threads = threads;
+    const int tile_log = a.lr + lc;
+    L.threads = threads ? threads : tile_log >= kMaxLogR ? 512 : tile_log >= 10 ? 256 : 128;
     if (half_total < L.threads) L.threads = half_total < 32 ? 32 : half_total;
     passes.push_back(L);
   }
@@ -937,11 +952,9 @@ static int run_ntt(const F& f, const zkb_field* field, const uint64_t* in, uint6
     return fail(ZKB_EWORKSPACE, "NTT of %lld rows needs %zu workspace bytes, got %zu",
                 (long long)n, need, ws_bytes);
   }
-  int sms = 0;
-  ZKB_TRY(sm_count(device, &sms));
   std::vector<PassLaunch> passes;
-  plan_passes(n, log_n, invert, rt, st, in, out, reinterpret_cast<uint64_t*>(workspace), sms, 0,
-              0, passes);
+  plan_passes(n, log_n, invert, rt, st, in, out, reinterpret_cast<uint64_t*>(workspace), 0, 0,
+              false, passes);
   const int P = (int)passes.size();
   for (int q = 0; q < P; ++q) {
     if (!passes[q].a.last) {
@@ -1024,7 +1037,7 @@ static int run_ntt_batch(const F& f, const zkb_field* field, const zkb_ntt_job* 
     const int log_n = ilog2(J.n);
     ZKB_TRY(lookup_tables(f, table_key(field, nullptr, log_n, device), J.n, log_n, J.invert,
                           J.has_coset ? J.coset : nullptr, rts[k], sts[k], s));
-    for (int r : plan_radices(log_n)) max_lr = std::max(max_lr, r);
+    for (int r : plan_radices(log_n, true)) max_lr = std::max(max_lr, r);
   }
   // one tile shape for every pass: 2^max(10, largest radix) rows, 256 threads
   const int cta_log = std::max(10, max_lr);
@@ -1032,8 +1045,8 @@ static int run_ntt_batch(const F& f, const zkb_field* field, const zkb_ntt_job* 
   for (size_t k = 0; k < order.size(); ++k) {
     const zkb_ntt_job& J = jobs[order[k]];
     plan_passes(J.n, ilog2(J.n), J.invert, rts[k], sts[k], J.in, J.out,
-                reinterpret_cast<uint64_t*>(ws + L.off_tmp[order[k]]), sms, cta_log,
-                kBatchThreads, plans[k]);
+                reinterpret_cast<uint64_t*>(ws + L.off_tmp[order[k]]), cta_log, kBatchThreads,
+                true, plans[k]);
   }
   // tile numbering: pass q of every transform before pass q + 1 of any
   size_t smem = 0;

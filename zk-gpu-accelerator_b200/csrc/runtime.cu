@@ -26,7 +26,7 @@ static Knob g_knobs[] = {
     {"msm.reduce_log_segment", 2, 1, 8},     // log2 of the running-sum segment length
     {"msm.call_products", 1, 0, 1},          // bucket kernels call one shared product (1) or inline all (0)
     {"msm.sort", 1, 0, 1},                   // pairs grouped by a counting sort (1) or a radix sort (0)
-    {"ntt.max_log_radix", 12, 8, 12},        // largest sub-transform per pass (log2)
+    {"ntt.max_log_radix", 0, 0, 12},         // largest sub-transform per pass (log2, 8..12; 0 = by size)
     {"ntt.cta_log_elems", 0, 0, 12},         // elements staged per CTA (log2, 9..12; 0 = by size)
     {"ntt.threads", 0, 0, 512},              // threads per NTT CTA (64..512; 0 = by tile)
     {"ntt.call_products", 0, 0, 1},          // pass kernels call one shared product (1) or inline all (0)
