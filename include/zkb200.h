@@ -323,7 +323,9 @@ int zkb_msm_fixed_batch(const zkb_msm_job* jobs, int count, void* workspace, siz
 /* ---- measurement -------------------------------------------------------- */
 
 /* Tuning knobs, read by each call when it plans its work (so they also change
- * the workspace size queries): "msm.pairs_per_thread" (default 64),
+ * the workspace size queries): "msm.pairs_per_thread" (sorted pairs a bucket
+ * thread adds in turn, 8..4096; default 0 = by size: the pair bound over 2^19,
+ * as a power of two within 8..64),
  * "msm.slots_per_thread" (8), "msm.reduce_log_segment" (2), "msm.sort" (1:
  * pairs grouped by a counting sort that skips zero digits; 0: a radix sort
  * of all pairs; the same points either way),

@@ -757,7 +757,7 @@ struct MsmPlan {
   int w = 0, W = 0, key_bits = 0;
   uint32_t none = 0;
   int64_t nb = 0;  // buckets per window
-  int k1 = 64;     // sorted pairs per bucket thread ("msm.pairs_per_thread")
+  int k1 = 64;     // sorted pairs per bucket thread ("msm.pairs_per_thread", else by size)
   int k2 = 8;      // slots per merge thread ("msm.slots_per_thread")
   int log_l = 2;   // log2 running-sum segment ("msm.reduce_log_segment")
   int call_products = 1;  // bucket kernels call one shared product ("msm.call_products")
@@ -776,7 +776,7 @@ struct MsmPlan {
 };
 
 // Plan for a batch of jobs with point counts sizes[0..count) at window w.
-static int make_plan(const int64_t* sizes, int count, int w, MsmPlan& p, int table = 0) {
+static int make_plan(const int64_t* sizes, int count, int w, MsmPlan& p, int table = 0, int k1 = 0) {
   p.count = count;
   p.first.assign(count + 1, 0);
   for (int j = 0; j < count; ++j) p.first[j + 1] = p.first[j] + sizes[j];
@@ -795,7 +795,19 @@ static int make_plan(const int64_t* sizes, int count, int w, MsmPlan& p, int tab
   p.keys_used = keys_used;
   p.counting_sort = table ? 1 : tune_get("msm.sort");
   p.E = 2 * (int64_t)p.W * n;  // both GLV halves
-  p.k1 = tune_get("msm.pairs_per_thread");
+  // pairs per level-1 thread: the knob, else by size. A thread adds its pairs one
+  // after another, so small MSMs want short chains and many threads; each thread
+  // may leave two partial sums for the merge levels, so large ones want long
+  // chains. E / 2^19 rounded down to a power of two, within 8..64: measured on
+  // B200 (uniform scalars, default windows), 8 pairs against 64 take 2^10 points
+  // from 1.89 to 1.56 ms, 2^14 from 2.07 to 1.79, 2^16 from 2.36 to 2.14; from
+  // 2^19 points 16-32 pairs match 64 (skewed scalars gain 5-12 %), and 2^21 up
+  // keeps 64.
+  p.k1 = k1 > 0 ? k1 : tune_get("msm.pairs_per_thread");
+  if (p.k1 < 8) {
+    p.k1 = 8;
+    while (p.k1 < 64 && ((int64_t)p.k1 << 20) <= p.E) p.k1 <<= 1;
+  }
   p.k2 = tune_get("msm.slots_per_thread");
   p.log_l = tune_get("msm.reduce_log_segment");
   p.call_products = tune_get("msm.call_products");
@@ -1335,6 +1347,11 @@ int zkb_msm_no_alloc(const uint64_t* points, const uint64_t* scalars, int64_t n,
   const int w = window_size ? window_size : default_window(n);
   MsmPlan p;
   ZKB_TRY(make_plan(&n, 1, w, p));
+  // the size-based chains of a small MSM leave more partial sums: when those do
+  // not fit the fixed scratch, the 64-pair chains of large MSMs may
+  if (p.total > kNoAllocScratchBytes && p.k1 < 64 && tune_get("msm.pairs_per_thread") < 8) {
+    ZKB_TRY(make_plan(&n, 1, w, p, 0, 64));
+  }
   if (p.total > kNoAllocScratchBytes) {
     return fail(ZKB_EWORKSPACE,
                 "MSM of %lld points at window %d needs %zu bytes of scratch; the library's fixed "

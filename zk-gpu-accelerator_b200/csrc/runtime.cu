@@ -21,7 +21,7 @@ struct Knob {
   int value, lo, hi;
 };
 static Knob g_knobs[] = {
-    {"msm.pairs_per_thread", 64, 8, 4096},   // sorted pairs each bucket thread adds
+    {"msm.pairs_per_thread", 0, 0, 4096},    // sorted pairs each bucket thread adds (8..4096; 0 = by size)
     {"msm.slots_per_thread", 8, 4, 4096},    // partial sums each merge thread adds
     {"msm.reduce_log_segment", 2, 1, 8},     // log2 of the running-sum segment length
     {"msm.call_products", 1, 0, 1},          // bucket kernels call one shared product (1) or inline all (0)
