@@ -673,9 +673,11 @@ __global__ void __launch_bounds__(128) k_msm_reduce(const uint64_t* X, const uin
 // 5. finalize
 // ---------------------------------------------------------------------------
 
-// One thread per job. Horner from the top window: acc = 2^w acc + S_win; then
-// affine x = X / ZZ, y = Y / ZZZ with one inversion of ZZ ZZZ, as plain
-// canonical values.
+// One thread per job. Horner from the top window: acc = 2^w acc + S_win, the w
+// doublings in Jacobian coordinates (7 products each against 9 in XYZZ; the
+// conversions cost 6 a window), the additions in XYZZ; then affine
+// x = X / ZZ, y = Y / ZZZ with one inversion of ZZ ZZZ, as plain canonical
+// values.
 template <class Mul>
 __global__ void k_msm_finalize(const MsmJobs J, const uint64_t* all_window_sums, int W, int w) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -686,7 +688,10 @@ __global__ void k_msm_finalize(const MsmJobs J, const uint64_t* all_window_sums,
   Xyzz acc, s;
   xyzz_load(acc, window_sums + 16 * (W - 1));
   for (int win = W - 2; win >= 0; --win) {
-    for (int k = 0; k < w; ++k) xyzz_dbl<Mul>(acc, acc);
+    Jac j;
+    xyzz_to_jac<Mul>(j, acc);
+    for (int k = 0; k < w; ++k) jac_dbl_m<Mul>(j, j);
+    jac_to_xyzz<Mul>(acc, j);
     xyzz_load(s, window_sums + 16 * win);
     xyzz_add<Mul>(acc, acc, s);
   }
