@@ -764,7 +764,7 @@ struct MsmPlan {
   int64_t nb = 0;  // buckets per window
   int k1 = 64;     // sorted pairs per bucket thread ("msm.pairs_per_thread", else by size)
   int k2 = 8;      // slots per merge thread ("msm.slots_per_thread")
-  int log_l = 2;   // log2 running-sum segment ("msm.reduce_log_segment")
+  int log_l = 1;   // log2 running-sum segment ("msm.reduce_log_segment")
   int call_products = 1;  // bucket kernels call one shared product ("msm.call_products")
   int counting_sort = 1;  // counting sort (1) or radix sort (0) of the pairs ("msm.sort")
   int table = 0;          // points are fixed-base tables: one bucket set per job
@@ -781,7 +781,8 @@ struct MsmPlan {
 };
 
 // Plan for a batch of jobs with point counts sizes[0..count) at window w.
-static int make_plan(const int64_t* sizes, int count, int w, MsmPlan& p, int table = 0, int k1 = 0) {
+static int make_plan(const int64_t* sizes, int count, int w, MsmPlan& p, int table = 0, int k1 = 0,
+                     int log_l = 0) {
   p.count = count;
   p.first.assign(count + 1, 0);
   for (int j = 0; j < count; ++j) p.first[j + 1] = p.first[j] + sizes[j];
@@ -814,7 +815,7 @@ static int make_plan(const int64_t* sizes, int count, int w, MsmPlan& p, int tab
     while (p.k1 < 64 && ((int64_t)p.k1 << 20) <= p.E) p.k1 <<= 1;
   }
   p.k2 = tune_get("msm.slots_per_thread");
-  p.log_l = tune_get("msm.reduce_log_segment");
+  p.log_l = log_l > 0 ? log_l : tune_get("msm.reduce_log_segment");
   p.call_products = tune_get("msm.call_products");
   p.T1 = (p.E + p.k1 - 1) / p.k1;
   p.slot_levels.clear();
@@ -1352,10 +1353,11 @@ int zkb_msm_no_alloc(const uint64_t* points, const uint64_t* scalars, int64_t n,
   const int w = window_size ? window_size : default_window(n);
   MsmPlan p;
   ZKB_TRY(make_plan(&n, 1, w, p));
-  // the size-based chains of a small MSM leave more partial sums: when those do
-  // not fit the fixed scratch, the 64-pair chains of large MSMs may
-  if (p.total > kNoAllocScratchBytes && p.k1 < 64 && tune_get("msm.pairs_per_thread") < 8) {
-    ZKB_TRY(make_plan(&n, 1, w, p, 0, 64));
+  // short bucket chains and two-bucket reduction segments, which suit small
+  // MSMs, take more scratch: when the plan does not fit the fixed scratch, the
+  // compact shape (at least 64 pairs per thread, 4-bucket segments) may
+  if (p.total > kNoAllocScratchBytes && (p.k1 < 64 || p.log_l < 2)) {
+    ZKB_TRY(make_plan(&n, 1, w, p, 0, p.k1 > 64 ? p.k1 : 64, p.log_l > 2 ? p.log_l : 2));
   }
   if (p.total > kNoAllocScratchBytes) {
     return fail(ZKB_EWORKSPACE,

@@ -23,7 +23,7 @@ struct Knob {
 static Knob g_knobs[] = {
     {"msm.pairs_per_thread", 0, 0, 4096},    // sorted pairs each bucket thread adds (8..4096; 0 = by size)
     {"msm.slots_per_thread", 8, 4, 4096},    // partial sums each merge thread adds
-    {"msm.reduce_log_segment", 2, 1, 8},     // log2 of the running-sum segment length
+    {"msm.reduce_log_segment", 1, 1, 8},     // log2 of the running-sum segment length
     {"msm.call_products", 1, 0, 1},          // bucket kernels call one shared product (1) or inline all (0)
     {"msm.sort", 1, 0, 1},                   // pairs grouped by a counting sort (1) or a radix sort (0)
     {"ntt.max_log_radix", 0, 0, 12},         // largest sub-transform per pass (log2, 8..12; 0 = by size)
