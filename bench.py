@@ -94,13 +94,14 @@ _GLV_G1 = 0x2D91D232EC7E0B3D7
 _GLV_G2 = 0x24CCEF014A773D2CF7A7BD9D4391EB18E
 
 
-def ntt_products(n: int, log_n: int) -> int:
+def ntt_products(n: int, log_n: int, passes: int | None = None) -> int:
     """Montgomery products of one forward NTT of n = 2^log_n rows as csrc/ntt.cu runs it: log_n
-    split into P passes (three from 2^19, else at most 12 bits each and two from 2^10); a pass of
-    2^lr rows does lr / 2 radix-4 rounds, the first with only the w_4 product (1 per 4 rows), the
-    others 4 per 4 rows, plus a radix-2 stage (1 per 2 rows) for odd lr; each pass boundary 1
-    product per row (the twiddle read from the expanded table)."""
-    P = 3 if log_n >= 19 else max(-(-log_n // 12), 2 if log_n >= 10 else 1)
+    split evenly into P passes (`passes`, else the library's default plan: three from 2^19, else
+    at most 12 bits each and two from 2^10); a pass of 2^lr rows does lr / 2 radix-4 rounds, the
+    first with only the w_4 product (1 per 4 rows), the others 4 per 4 rows, plus a radix-2 stage
+    (1 per 2 rows) for odd lr; each pass boundary 1 product per row (the twiddle read from the
+    expanded table)."""
+    P = passes or (3 if log_n >= 19 else max(-(-log_n // 12), 2 if log_n >= 10 else 1))
     radices = [log_n // P + (1 if q < log_n % P else 0) for q in range(P)]
     per_row = 0.0
     for lr in radices:
@@ -449,7 +450,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     n_passes = sum(v[0] for k, v in prof_ntt.items() if k.startswith("ntt_")) / max(2, min(args.steps, 5))
     ntt_bytes = 64 * step.m * n_passes
     ntt_gbs = ntt_bytes / (ntt_pass_ms * 1e-3) / 1e9
-    ntt_mulmods = ntt_products(step.m, log_ntt)
+    ntt_mulmods = ntt_products(step.m, log_ntt, round(n_passes) or None)
     ntt_roof = {"bytes_per_launch": int(ntt_bytes), "ms": round(ntt_pass_ms, 4), "achieved_gbs": round(ntt_gbs, 1),
                 "hbm_frac": round(ntt_gbs / hbm_peak, 4) if hbm_peak else None,
                 "imad_frac": round(ntt_mulmods * IMAD_PER_MULMOD / (ntt_pass_ms * 1e-3) / 1e12 / imad_peak_t, 4),

@@ -91,3 +91,14 @@ def test_glv_halves_recombine(w):
         k1 = k - c1 * bench._GLV_A1 - c2 * bench._GLV_A2
         k2 = c1 * bench._GLV_B1_ABS - c2 * bench._GLV_A1
         assert (k1 + k2 * lam - k) % po.R == 0
+
+
+def test_ntt_product_count_follows_the_pass_plan():
+    """Products per row of the NTT the roofline counts: 12 radix-4 rounds over two 12-bit passes
+    (11.5 per row at 2^24) or three 8-bit passes (11.75), the default plan from 2^19 rows."""
+    n = 1 << 24
+    assert bench.ntt_products(n, 24, 2) == int(11.5 * n)
+    assert bench.ntt_products(n, 24, 3) == int(11.75 * n)
+    assert bench.ntt_products(n, 24) == bench.ntt_products(n, 24, 3)
+    assert bench.ntt_products(1 << 16, 16) == bench.ntt_products(1 << 16, 16, 2) == int(7.5 * (1 << 16))
+    assert bench.ntt_products(1 << 9, 9) == int(((0.25 + 3) + 0.5) * (1 << 9))  # one pass, odd radix
