@@ -30,10 +30,16 @@ NTT and a 2^26-word element-wise product, with their HBM rooflines.
 
 --impl reference runs the reference's CPU algorithms (the same C port, all
 host threads) on the same workload and prints the same line with
-"impl": "reference".
+"impl": "reference". Both arms print `outputs_sha256`, a digest of the step's
+four results, and our arm checks the timed results bit for bit against the
+C port at full size (`parity_full`).
 
-N > 1 (torchrun): every rank runs its own instance of the step (weak
-scaling, no collective on the data path); the time is the max over ranks.
+N > 1: under torchrun, or started here when --gpus N > 1 and no launcher set
+WORLD_SIZE (one process per GPU, rendezvous on 127.0.0.1). Every rank runs
+its own instance of the step (weak scaling, no collective on the data path);
+the time is the max over ranks. Beside it, `sharded` times one MSM and one
+NTT split over the ranks (strong scaling, NCCL exchanges). --check-ranks runs
+only the multi-rank plumbing (gloo on a machine without GPUs).
 """
 
 from __future__ import annotations
@@ -65,6 +71,34 @@ WORKLOADS = {
 }
 
 
+def workload_config(log_msm: int, log_ntt: int, world: int) -> dict:
+    """The `config` object of both arms' lines: what the step computes, on which inputs
+    (implementation choices such as the window go under `impl_config`)."""
+    return {"workload": f"msm-2^{log_msm}-uniform+skewed, ntt-2^{log_ntt}+coset",
+            "msm_points": 1 << log_msm, "ntt_size": 1 << log_ntt, "coset": COSET,
+            "scalars": ["uniform [0,r)", "skewed 60% {0,1} / 20% < 2^32 / 20% uniform"],
+            "seeds": {"bases": 10, "uniform": 11, "skewed": 12, "ntt": 13, "per_rank_offset": 100},
+            "l2": "every input larger than the 126 MB L2 (bases 256 MiB, NTT 512 MiB)"
+                  if log_msm >= 22 else "small inputs",
+            "parallelism": f"replicas x{world}"}
+
+
+def outputs_sha256(msm_uniform, msm_skewed, ntt_plain, ntt_coset) -> str:
+    """SHA-256 over one step's results: the two MSM results as 9 little-endian uint64 each
+    (plain affine x, y, then the infinity flag) and the two transforms' Montgomery rows.
+    Both arms hash the same bytes, so equal digests mean identical outputs."""
+    import hashlib
+
+    import numpy as np
+
+    h = hashlib.sha256()
+    for a in (msm_uniform, msm_skewed):
+        h.update(np.ascontiguousarray(np.asarray(a, dtype=np.uint64).reshape(-1)[:9]).tobytes())
+    for a in (ntt_plain, ntt_coset):
+        h.update(np.ascontiguousarray(np.asarray(a).view(np.uint64)).tobytes())
+    return h.hexdigest()
+
+
 def _peaks() -> dict:
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -83,6 +117,7 @@ IMAD_PER_MULMOD = 264  # 2 x 64 32-bit multiply-adds (lo and hi) for a*b and m*p
 IMAD_PER_SQR = 208     # 2 x (36 + 64) for a*a (each cross product once) and m*p, plus 8 for the m's
 # XYZZ mixed addition: 8 multiplications + 2 squarings
 IMAD_PER_MADD = 8 * IMAD_PER_MULMOD + 2 * IMAD_PER_SQR
+PRODUCTS_PER_MADD = 10
 
 
 # GLV split constants (csrc/msm.cu): k = k1 + k2 lambda, c1 = floor(k g1 / 2^256), ...
@@ -217,6 +252,68 @@ class ClockSampler:
 
 def dist_env() -> tuple[int, int, int]:
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def _free_port() -> int:
+    import socket
+
+    with socket.socket() as sock:
+        sock.bind(("127.0.0.1", 0))
+        return sock.getsockname()[1]
+
+
+def spawn_ranks(n: int, argv: list[str], timeout_s: float | None = None) -> int:
+    """`python bench.py --gpus N` without a launcher: start N copies of this script as
+    ranks 0..N-1 (one per GPU, LOCAL_RANK = RANK) with the torch.distributed rendezvous
+    on 127.0.0.1, pass rank 0's output through, and return the worst exit code. If a rank
+    fails, the others are stopped (by their own process handles) instead of waiting on a
+    collective that will not complete."""
+    port = _free_port()
+    procs = []
+    for r in range(n):
+        env = dict(os.environ, RANK=str(r), LOCAL_RANK=str(r), WORLD_SIZE=str(n), LOCAL_WORLD_SIZE=str(n),
+                   MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+        procs.append(subprocess.Popen([sys.executable, str(Path(__file__).resolve()), *argv], env=env,
+                                      stdout=None if r == 0 else subprocess.DEVNULL))
+    deadline = None if timeout_s is None else time.monotonic() + timeout_s
+    codes: dict[int, int] = {}
+    while len(codes) < n:
+        for r, p in enumerate(procs):
+            if r not in codes and p.poll() is not None:
+                codes[r] = p.returncode
+        if any(c != 0 for c in codes.values()) or (deadline is not None and time.monotonic() > deadline):
+            for r, p in enumerate(procs):
+                if r not in codes:
+                    p.kill()
+                    codes[r] = p.wait() or 1
+            break
+        time.sleep(0.05)
+    return max(abs(c) for c in codes.values())
+
+
+def check_ranks(args, rank: int, world: int, local_rank: int) -> dict | None:
+    """The multi-rank plumbing alone (process group, barrier, max over ranks, a gather
+    of every rank's identity), on the GPUs with NCCL or on the CPU with gloo."""
+    import torch
+
+    cuda = torch.cuda.is_available()
+    if cuda:
+        torch.cuda.set_device(local_rank)
+    device = torch.device("cuda", local_rank) if cuda else torch.device("cpu")
+    dist = init_dist(world, "nccl" if cuda else "gloo")
+    barrier(dist, device)
+    worst = max_over_ranks(float(rank + 1), dist, device)
+    ident = torch.tensor([rank, local_rank, os.getpid()], dtype=torch.int64, device=device)
+    if dist is not None:
+        everyone = [torch.zeros_like(ident) for _ in range(world)]
+        dist.all_gather(everyone, ident)
+        dist.destroy_process_group()
+    else:
+        everyone = [ident]
+    if rank != 0:
+        return None
+    return {"check": "ranks", "n_gpus": world, "gpus_requested": args.gpus, "backend": "nccl" if cuda else "gloo",
+            "ranks": [[int(v) for v in t.tolist()[:2]] for t in everyone], "max_over_ranks": worst}
 
 
 def init_dist(world: int, backend: str):
@@ -392,6 +489,11 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     part_ms = {name: sum(ev[k][j].elapsed_time(ev[k][j + 1]) for k in range(reps)) / reps
                for j, (name, _) in enumerate(parts)}
     same = step.same_results()
+    # the timed step's own outputs (the batched step's results), hashed as the reference arm hashes its own
+    plan_outs = [step.plan.msm_results[0, :9].cpu().numpy().view(np.uint64),
+                 step.plan.msm_results[1, :9].cpu().numpy().view(np.uint64),
+                 step.plan.ntt_outputs[0].cpu().numpy(), step.plan.ntt_outputs[1].cpu().numpy()]
+    digest = outputs_sha256(*plan_outs)
 
     # ---- stage profile (library-recorded CUDA events on the launch stream), separate steps
     _native.profile_enable(True)
@@ -424,9 +526,13 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         imad = madds * IMAD_PER_MADD
         achieved = imad / (ms * 1e-3) / 1e12
         acc_bytes = madds * (64 + 8) + 2 * (-(-madds // 64)) * 132  # point gathers + sorted pairs + slots
+        products = madds * PRODUCTS_PER_MADD
         return {
             "kernel": kernel, "bound": "imad", "achieved": round(achieved, 3), "peak": round(imad_peak_t, 3),
             "unit": "TIMAD/s", "frac": round(achieved / imad_peak_t, 4), "traffic": traffic,
+            "peak_measured": peak_measured, "frac_of_measured": round(achieved / imad_meas_t, 4),
+            "products_per_s": round(products / (ms * 1e-3) / 1e9, 3),
+            "products_frac_of_measured": round(products / (ms * 1e-3) / prod_meas, 4),
             "peak_source": f"nominal issue rate: {sm_count} SMs x 64 IMAD/clk x {mhz:.0f} MHz (median SM clock "
                            "sampled in the timed region)",
             "work_per_launch": f"{madds} mixed additions x (8 x {IMAD_PER_MULMOD} + 2 x {IMAD_PER_SQR}) IMAD",
@@ -435,6 +541,18 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
                     "frac": round(acc_bytes / (ms * 1e-3) / 1e9 / hbm_peak, 4) if hbm_peak else None,
                     "source": "measured (MEASURED_PEAKS.json)" if hbm_peak else None},
         }
+
+    measured = _native.measure_int_peaks()
+    imad_meas_t = measured["madlo_per_clk_sm"] * sm_count * mhz * 1e6 / 1e12
+    prod_meas = measured["montmul_per_clk_sm"] * sm_count * mhz * 1e6  # Montgomery products / s
+    peak_measured = {
+        "imad_t_per_s": round(imad_meas_t, 3), "montmul_per_s": round(prod_meas / 1e9, 3),
+        "unit": "T IMAD/s; G products/s", "at_mhz": mhz,
+        "per_clk_sm": {k: round(measured[f"{k}_per_clk_sm"], 3) for k in ("madlo", "madwide", "montmul")},
+        "probe_mhz": {k: round(measured[f"{k}_mhz"], 1) for k in ("madlo", "madwide", "montmul")},
+        "source": "zkb_measure_int_peaks (csrc/peak.cu): one-wave loops of independent mad.lo.u32, "
+                  "mad.wide.u32 and 256-bit Montgomery products, SM cycle counters; scaled to the clock "
+                  "sampled in the timed region"}
 
     traffic_u = _profile_traffic("k_msm_acc_points", step.n)
     traffic_s = _profile_traffic("k_msm_acc_points_skewed", step.n)
@@ -470,9 +588,16 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     if args.workload == "large" and not args.skip_int64:
         int64 = run_int64(cpu=rank == 0 and not args.skip_cpu_baseline)
 
+    sharded = None
+    if world > 1:
+        sharded = run_sharded(args, step, dist, device, rank, world, log_msm, log_ntt)
+
     cpu = None
     if rank == 0 and not args.skip_cpu_baseline:
         cpu = cpu_baseline_sample(step, threads=1)
+    parity = None
+    if rank == 0 and not args.skip_parity:
+        parity = full_size_parity(step, plan_outs, digest)
 
     if dist is not None:
         dist.destroy_process_group()
@@ -482,14 +607,15 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         "metric": METRIC, "value": round(ms_step, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_step, 3), "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32 (8x32-bit limb Montgomery, exact)", "data": "synthetic (seeded)",
-        "config": {"workload": f"msm-2^{log_msm}-uniform+skewed, ntt-2^{log_ntt}+coset",
-                   "msm_points": step.n, "msm_window": step.w, "ntt_size": step.m, "coset": COSET,
-                   "scalars": ["uniform [0,r)", "skewed 60% {0,1} / 20% < 2^32 / 20% uniform"],
-                   "l2": "every input larger than the 126 MB L2 (bases 256 MiB, NTT 512 MiB)",
-                   "parallelism": f"replicas x{world}",
-                   "schedule": "one MSM batch (both MSMs, one pipeline) on a high-priority stream; both "
-                               "transforms as pass launches (zkb_ntt each) on a low-priority stream beside it",
-                   **({"knobs": dict(kv.split("=", 1) for kv in args.knob)} if args.knob else {})},
+        "config": workload_config(log_msm, log_ntt, world),
+        "impl_config": {"msm_window": step.w,
+                        "schedule": "one MSM batch (both MSMs, one pipeline) on a high-priority stream; both "
+                                    "transforms as pass launches (zkb_ntt each) on a low-priority stream "
+                                    "beside it",
+                        **({"knobs": dict(kv.split("=", 1) for kv in args.knob)} if args.knob else {})},
+        "outputs_sha256": digest,
+        "parity_full": parity,
+        "sharded": sharded,
         "parts_ms": {k: round(v, 3) for k, v in part_ms.items()},
         "msm_points_per_s": {k: round(step.n / (v * 1e-3)) for k, v in part_ms.items() if k.startswith("msm")},
         "sequential_ms": round(sum(part_ms.values()), 3),
@@ -654,6 +780,78 @@ def _run_e2e(args, step: Step, dist, device, log_msm: int, log_ntt: int) -> dict
                    "host threads on four streams, inputs staged on one copy stream, MSM inputs first (the "
                    "base set copied once), then the NTT inputs; NTTs on high-priority streams; api_copies_ms: the same calls "
                    "given the host tensors (each copies its own inputs); sequential_ms: one after another"}
+
+
+def full_size_parity(step: Step, plan_outs: list, digest: str) -> dict:
+    """The timed step's four results against the C port of the reference's CPU algorithms
+    at full size (all host threads): bit for bit, and by the same SHA-256 the reference
+    arm prints."""
+    import numpy as np
+
+    threads = os.cpu_count() or 1
+    bases_h = step.bases.cpu().numpy()
+    ntt_h = step.ntt_in.cpu().numpy()
+    outs, secs = oracle_outputs(bases_h, step.sc_uniform_host, step.sc_skewed_host, ntt_h, threads)
+    same = [bool(np.array_equal(np.asarray(a, dtype=np.uint64).reshape(-1)[:9], b.reshape(-1)[:9]))
+            for a, b in zip(outs[:2], plan_outs[:2])]
+    same += [bool(np.array_equal(np.asarray(a).view(np.uint64), np.asarray(b).view(np.uint64)))
+             for a, b in zip(outs[2:], plan_outs[2:])]
+    oracle_digest = outputs_sha256(*outs)
+    return {"same": all(same) and oracle_digest == digest,
+            "parts": dict(zip(("msm_uniform", "msm_skewed", "ntt", "coset_ntt"), same)),
+            "oracle_sha256": oracle_digest, "oracle_s": round(secs, 2), "threads": threads,
+            "oracle": "C port of the reference's CPU Pippenger and Radix-2 NTT (oracle/zk_oracle.c), full size"}
+
+
+def run_sharded(args, step: Step, dist, device, rank: int, world: int, log_msm: int, log_ntt: int) -> dict:
+    """Strong scaling beside the replicas: ONE 2^log_msm uniform MSM with its points split
+    over the ranks (each rank's partial sum, one all-gather of 72-byte results) and ONE
+    2^log_ntt NTT split four-step over the ranks (two all-to-all exchanges, cyclic output),
+    both over NCCL (zkgpu.sharded). Device time per operation with CUDA events, max over
+    ranks. Rank 0's results are checked against its own one-GPU results of the same
+    inputs (rank 0's replica uses the same seeds)."""
+    import numpy as np
+    import torch
+
+    from zkgpu import curve_gpu, sharded, workloads as wl
+    from zkgpu.field256_gpu import BN254_FR
+
+    n, m = 1 << log_msm, 1 << log_ntt
+    lo, hi = sharded.shard_bounds(n, world, rank)
+    pts = curve_gpu.mul_generator(wl.base_scalars(10, n)[lo:hi])
+    sc = torch.from_numpy(np.ascontiguousarray(wl.uniform_fr(11, n)[lo:hi])).to(device)
+    mlo, mhi = sharded.shard_bounds(m, world, rank)
+    x = BN254_FR.to_montgomery(np.ascontiguousarray(wl.uniform_fr(13, m)[mlo:mhi]))
+    torch.cuda.synchronize()
+    reps = 3
+
+    def timed(fn) -> tuple[float, object]:
+        out = None
+        for _ in range(2):
+            out = fn()
+        torch.cuda.synchronize()
+        barrier(dist, device)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            out = fn()
+        b.record()
+        torch.cuda.synchronize()
+        return max_over_ranks(a.elapsed_time(b) / reps, dist, device), out
+
+    msm_ms, point = timed(lambda: sharded.msm_sharded(pts, sc, window_size=step.w))
+    ntt_ms, y = timed(lambda: sharded.ntt_sharded(x))
+    checks = None
+    if rank == 0:
+        from zkgpu.batch import results_to_points
+
+        one_gpu = results_to_points(step.plan.msm_results[:1])[0]
+        want = step.plan.ntt_outputs[0][0::world]  # rank 0's cyclic slice: y[0], y[G], ...
+        checks = {"msm_same_as_one_gpu": point == one_gpu, "ntt_slice_same_as_one_gpu": bool(torch.equal(y, want))}
+    return {"scaling": "strong", "ranks": world, "msm_ms": round(msm_ms, 3), "ntt_ms": round(ntt_ms, 3),
+            "msm": f"one 2^{log_msm} uniform MSM, {n // world}-point slices, one all-gather",
+            "ntt": f"one 2^{log_ntt} NTT, four-step over {world} ranks, two all-to-all exchanges (cyclic output)",
+            "timing": f"CUDA events, mean of {reps} after 2 warm-up, max over ranks", "checks": checks}
 
 
 # ------------------------------------------------------------------
@@ -967,12 +1165,29 @@ def cpu_baseline_sample(step: Step, threads: int) -> dict:
 # ------------------------------------------------------------------
 
 
+def oracle_outputs(bases_h, sc_u, sc_s, ntt_h, threads: int) -> tuple[list, float]:
+    """The step's four results from the C port of the reference's CPU algorithms, and the
+    seconds it took: MSMs at the reference's window for n (zkgpu/msm.py:112-121), the NTT and
+    the coset NTT (zkgpu/ntt.py:149-203, zkgpu/domain.py:122-135) on Montgomery rows."""
+    from oracle import c_oracle as co
+    from oracle import pyoracle as po
+
+    w = po.pippenger_window_size(bases_h.shape[0])
+    t0 = time.perf_counter()
+    outs = [co.msm(bases_h, sc_u, w, threads=threads), co.msm(bases_h, sc_s, w, threads=threads),
+            co.ntt(ntt_h, threads=threads), co.ntt(ntt_h, coset=COSET, threads=threads)]
+    return outs, time.perf_counter() - t0
+
+
 def run_reference(args, rank: int, world: int) -> dict | None:
-    """The reference's CPU algorithms (C port) on the same workload, all host threads."""
+    """The reference's CPU algorithms (C port, all host threads) on the same workload.
+
+    One untimed full step first (its outputs give `outputs_sha256`, comparable with the
+    GPU arm's), then exactly --steps timed steps: the whole step when --steps of them fit
+    in about 150 s at the full step's speed, else each step the bounded sample of
+    cpu_estimate (MSM windows 0-2 at full n, 2 NTT stages, scaled). Rank 0 alone runs."""
     if rank != 0:
         return None
-    import numpy as np
-
     from oracle import c_oracle as co
     from zkgpu import workloads as wl
 
@@ -983,29 +1198,29 @@ def run_reference(args, rank: int, world: int) -> dict | None:
     bases_h = co.mul_generator(k, threads=threads)
     sc_u, sc_s = wl.uniform_fr(11, n), wl.skewed_scalars(12, n)
     ntt_h = co.to_mont(co.FR, wl.uniform_fr(13, m))
-    # The whole step when the host has the threads for it (the MSM runs its
-    # windows in parallel, the NTT each stage's butterflies), else the bounded
-    # sample. One CPU step takes seconds, so at most 3 steps are timed after one
-    # warm-up, whatever --steps and --warmup ask for.
-    full = threads >= 8
-    warm, timed = min(args.warmup, 1), max(1, min(args.steps, 3))
+    outs, full_s = oracle_outputs(bases_h, sc_u, sc_s, ntt_h, threads)
+    digest = outputs_sha256(*outs)
+    steps = max(1, args.steps)
+    full = full_s * steps <= 150.0
+    for _ in range(max(0, args.warmup - 1)):  # the full step above was the first warm-up
+        cpu_estimate(bases_h, sc_u, sc_s, ntt_h, log_ntt, threads, full)
     times = []
     notes = ""
-    for i in range(warm + timed):
+    for _ in range(steps):
         ms, notes = cpu_estimate(bases_h, sc_u, sc_s, ntt_h, log_ntt, threads, full)
-        if i >= warm:
-            times.append(ms)
+        times.append(ms)
     value = statistics.mean(times)
     sample = ("full step" if full else "bounded sample (MSM windows 0-2 at full n, NTT 2 of "
-              f"{log_ntt} stages, scaled)") + f" with {threads} threads, mean of {timed} after {warm} warm-up; " + notes
+              f"{log_ntt} stages, scaled; the full step took {full_s:.1f} s)") + \
+        f" with {threads} threads, mean of {steps} timed steps; " + notes
     return {
         "impl": "reference", "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "steps_timed": timed, "ms_per_step": round(value, 1),
+        "steps": steps, "warmup": args.warmup, "steps_timed": steps, "ms_per_step": round(value, 1),
         "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "u64 (4x64-bit limb Montgomery, exact)",
         "data": "synthetic (seeded)",
-        "config": {"workload": f"msm-2^{log_msm}-uniform+skewed, ntt-2^{log_ntt}+coset", "msm_points": n,
-                   "ntt_size": m, "coset": COSET},
+        "config": workload_config(log_msm, log_ntt, world),
+        "outputs_sha256": digest,
         "cpu_baseline": {"value": round(value, 1), "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -1027,11 +1242,24 @@ def main() -> None:
                     help="set a library tuning knob (zkb_tune_set) before the run; repeatable")
     ap.add_argument("--tune", action="store_true",
                     help="measure (or load from the cache) per-size MSM windows and NTT shapes first")
+    ap.add_argument("--skip-parity", action="store_true",
+                    help="skip the full-size bit-exact check of the timed outputs against the C oracle")
+    ap.add_argument("--check-ranks", action="store_true",
+                    help="run only the multi-rank plumbing (spawn, process group, barrier, max over ranks)")
     args = ap.parse_args()
+    if args.gpus < 1:
+        ap.error("--gpus must be at least 1")
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # no launcher: start one rank per GPU here (torchrun sets WORLD_SIZE itself)
+        sys.exit(spawn_ranks(args.gpus, sys.argv[1:]))
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3  # at least three untimed steps
     rank, world, local_rank = dist_env()
-    if args.impl == "reference":
+    if world != args.gpus:
+        raise SystemExit(f"bench.py: --gpus {args.gpus} but the launcher started {world} ranks")
+    if args.check_ranks:
+        line = check_ranks(args, rank, world, local_rank)
+    elif args.impl == "reference":
         line = run_reference(args, rank, world)
     else:
         line = run_ours(args, rank, world, local_rank)

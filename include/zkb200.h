@@ -254,9 +254,11 @@ int zkb_msm(const uint64_t* points, const uint64_t* scalars, int64_t n, int wind
  * scratch is a fixed 64 MiB array inside the library (zkb_msm_no_alloc_capacity()),
  * which every GPU that loads the library keeps until the process exits. That
  * covers 2^16 points at the default window; a problem that needs more returns
- * ZKB_EWORKSPACE. The first call on each device looks up the array's device
- * address (with that device current); make that first call before any stream
- * capture. All calls share the array, so calls whose work overlaps on the GPU
+ * ZKB_EWORKSPACE. Each call looks up the array's device address for the
+ * current device; the first call on a device also loads the library's code
+ * there, so make that first call before any stream capture. A problem of 2^31
+ * or more digit pairs is refused with ZKB_EINVAL, as by zkb_msm (the 64 MiB
+ * limit refuses it first). All calls share the array, so calls whose work overlaps on the GPU
  * (other streams or other host threads) race: order them, e.g. on one stream.
  * Nothing is allocated or freed. */
 int zkb_msm_no_alloc(const uint64_t* points, const uint64_t* scalars, int64_t n, int window_size,
@@ -343,7 +345,11 @@ int zkb_msm_fixed_batch(const zkb_msm_job* jobs, int count, void* workspace, siz
  * "ntt.full_table_mb" (MiB the library may hold in expanded NTT tables: per
  * pass shape and direction the boundary twiddles of a non-last pass, per
  * coset transform its n scale factors, each saving one product per row;
- * default 4096, 0 = none).
+ * default 4096, 0 = none);
+ * "ntt.batch_spin_limit" (polls, each after a sleep of at least 256 ns, before
+ * a tile of zkb_ntt_batch gives up waiting for the previous pass of its
+ * transform and reports ZKB_ETIMEOUT through the status word; 0 = the default
+ * 2^22, about a second).
  * ZKB_EINVAL for an unknown name or a value out of range. Process-wide, not
  * per stream. */
 int zkb_tune_set(const char* key, int value);
@@ -361,6 +367,25 @@ int zkb_tune_get(const char* key, int* value);
  * between a workspace-size query and the call it sizes and the two disagree. */
 int zkb_tune_set_sized(const char* key, int log_n, int value);
 int zkb_tune_get_sized(const char* key, int log_n, int* value);
+
+/* Measured issue rates on the current device: loops of independent
+ * mad.lo.u32, of mad.wide.u32 (32 x 32 -> 64-bit multiply-add) and of this
+ * library's 256-bit Montgomery product over BN254's base field, each one
+ * launch of as many 256-thread blocks as fit the SMs at once. *_per_clk_sm is
+ * operations per SM per SM clock (from the SMs' cycle counters, independent
+ * of the clock), *_per_s per second over the whole GPU (CUDA events), *_mhz
+ * the SM clock that the two imply. They are the measured denominators of the
+ * integer rooflines; the IMAD pipe peak at clock f is sms * madlo_per_clk_sm
+ * * f. Takes a few tens of milliseconds and synchronises the stream. */
+typedef struct zkb_int_peaks {
+  double madlo_per_clk_sm, madlo_per_s, madlo_mhz;
+  double madwide_per_clk_sm, madwide_per_s, madwide_mhz;
+  double montmul_per_clk_sm, montmul_per_s, montmul_mhz;
+  int32_t sms;
+  int32_t reserved;
+} zkb_int_peaks;
+
+int zkb_measure_int_peaks(zkb_int_peaks* out, void* stream);
 
 /* Number of this library's own kernels launched so far in this process
  * (sorting kernels of the CUB library are not counted). */

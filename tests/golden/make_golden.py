@@ -1,10 +1,11 @@
 """
 Regenerate the golden fixtures in tests/golden/ by running the reference itself.
 
-    python tests/golden/make_golden.py [--reference /path/to/zk-gpu-accelerator] [--quick]
+    python tests/golden/make_golden.py --reference /path/to/zk-gpu-accelerator [--quick]
+    (or ZKGPU_REFERENCE=/path/to/zk-gpu-accelerator python tests/golden/make_golden.py)
 
 The reference (erihhh6/zk-gpu-accelerator) is pure Python, so its CPU path is
-imported directly from its source tree (default: /root/reference/src) and
+imported directly from the `src` folder of the checkout given and
 run on inputs regenerated from seeds by zkgpu/workloads.py (loaded by file
 path, since the reference's package is also named zkgpu). Only results are
 stored: big integers as hex strings, and for large transforms the SHA-256 of
@@ -30,6 +31,7 @@ import argparse
 import hashlib
 import importlib.util
 import json
+import os
 import random
 import sys
 import time
@@ -61,10 +63,13 @@ def rows_digest(values: list[int], mod: int, montgomery: bool = True) -> str:
 
 def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[1])
-    ap.add_argument("--reference", default="/root/reference", help="reference checkout")
+    ap.add_argument("--reference", default=os.environ.get("ZKGPU_REFERENCE"),
+                    help="checkout of the reference repository (or set ZKGPU_REFERENCE)")
     ap.add_argument("--quick", action="store_true", help="skip the 2^16 MSM and 2^20 NTT")
     ap.add_argument("--only", help="write this fixture file alone (field64.json)")
     args = ap.parse_args()
+    if not args.reference:
+        ap.error("give the reference checkout with --reference or ZKGPU_REFERENCE")
     sys.path.insert(0, str(Path(args.reference) / "src"))
     if args.only == "field64.json":
         field64_fixtures()

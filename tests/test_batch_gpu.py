@@ -185,3 +185,36 @@ def test_concurrent_plan_equals_the_sequential_plan_and_replays(base_set):
     torch.cuda.synchronize()
     assert all(bool((a == b).all()) for a, b in zip(seq.ntt_outputs, conc.ntt_outputs, strict=True))
     assert seq.msm_points_out() == conc.msm_points_out()
+
+
+# ------------------------------------------------------------------
+# The persistent launch's bounded dependency wait
+# ------------------------------------------------------------------
+
+
+def test_ntt_batch_wait_that_runs_out_reports_timeout_then_next_batch_is_exact():
+    """A tile of a transform's second pass waits for every tile of its first pass. With the
+    wait bounded to one poll ("ntt.batch_spin_limit" = 1), the first second-pass tile of a
+    2^22-row transform gives up while the last wave of first-pass tiles is still running: the
+    kernel returns, the status word reads ZKB_ETIMEOUT, and the host raises. The default bound
+    then gives the exact transform again (the counters and status are reset per launch)."""
+    import torch
+
+    x = _rows_fr(171, 1 << 22)
+    want = BN254_FR.ntt(x)
+    _native.tune_set("ntt.batch_spin_limit", 1)
+    try:
+        plan = batch.BatchPlan(ntt_jobs=[(x, False, None)])
+        plan.run()
+        torch.cuda.synchronize()
+        assert int(plan.status.item()) == _native.ZKB_ETIMEOUT
+        with pytest.raises(RuntimeError):
+            plan.check_status()
+    finally:
+        _native.tune_set("ntt.batch_spin_limit", 0)
+    assert _native.tune_get("ntt.batch_spin_limit") == 0
+    plan.run()
+    plan.check_status()
+    assert bool((plan.ntt_outputs[0] == want).all())
+    fresh = batch.ntt_batch([x])  # the functional form checks the status itself
+    assert bool((fresh[0] == want).all())

@@ -102,3 +102,46 @@ def test_ntt_product_count_follows_the_pass_plan():
     assert bench.ntt_products(n, 24) == bench.ntt_products(n, 24, 3)
     assert bench.ntt_products(1 << 16, 16) == bench.ntt_products(1 << 16, 16, 2) == int(7.5 * (1 << 16))
     assert bench.ntt_products(1 << 9, 9) == int(((0.25 + 3) + 0.5) * (1 << 9))  # one pass, odd radix
+
+
+def test_gpus_flag_starts_one_rank_per_gpu_without_a_launcher():
+    """`bench.py --gpus 2` with no torchrun environment starts two ranks itself; rank 0
+    prints the line and sees both ranks (gloo here, NCCL on GPUs)."""
+    import json
+    import subprocess
+
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK", "MASTER_PORT")}
+    env["CUDA_VISIBLE_DEVICES"] = ""
+    out = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--gpus", "2", "--check-ranks"], env=env,
+                         capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1  # rank 0 alone prints
+    line = json.loads(lines[0])
+    assert line["n_gpus"] == 2 and line["gpus_requested"] == 2 and line["backend"] == "gloo"
+    assert line["ranks"] == [[0, 0], [1, 1]]
+    assert line["max_over_ranks"] == 2.0
+
+
+def test_gpus_flag_must_match_the_launcher():
+    import subprocess
+
+    env = dict(os.environ, RANK="0", WORLD_SIZE="1", LOCAL_RANK="0", CUDA_VISIBLE_DEVICES="")
+    out = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--gpus", "2", "--check-ranks"], env=env,
+                         capture_output=True, text=True, timeout=300)
+    assert out.returncode != 0 and "--gpus 2" in out.stderr
+
+
+def test_reference_arm_times_every_requested_step_and_hashes_its_outputs():
+    from oracle import c_oracle as co
+    from zkgpu import workloads as wl
+
+    line = bench.run_reference(SimpleNamespace(workload="tiny", steps=4, warmup=1), 0, 1)
+    assert line["steps"] == 4 and line["steps_timed"] == 4
+    assert line["config"] == bench.workload_config(10, 10, 1)
+    # the digest is that of the C port's outputs on the seeded inputs
+    n = 1 << 10
+    bases = co.mul_generator(wl.base_scalars(10, n), threads=2)
+    ntt_h = co.to_mont(co.FR, wl.uniform_fr(13, n))
+    outs, _ = bench.oracle_outputs(bases, wl.uniform_fr(11, n), wl.skewed_scalars(12, n), ntt_h, 2)
+    assert line["outputs_sha256"] == bench.outputs_sha256(*outs)

@@ -1304,24 +1304,23 @@ namespace zkb {
 
 static constexpr size_t kNoAllocScratchBytes = 64ull << 20;
 static __device__ __align__(256) unsigned char g_msm_static_scratch[kNoAllocScratchBytes];
+// The sort's key and value arrays take 16 bytes per digit pair, so no plan that
+// fits the array can reach the 2^31 pairs the sort indexes (checked again below).
+static_assert(kNoAllocScratchBytes < (1ull << 31) * 16, "the fixed scratch could hold 2^31 sort pairs");
 
-// Device address of g_msm_static_scratch per device, looked up once per device
-// (with that device current) on the first call there.
-static std::mutex g_static_scratch_mutex;
-static void* g_static_scratch_addr[64] = {};
-
+// Device address of g_msm_static_scratch for the current device and context.
+// In host code the array's name is only a host-side stand-in; the address a
+// kernel may use comes from cudaGetSymbolAddress with the device current. It is
+// looked up on every call (a table lookup in the runtime, no allocation) rather
+// than cached per device index: after cudaDeviceReset, or under another context
+// on the same device, a cached address would point into a module that no longer
+// exists. The first lookup on a device also loads the library's module there.
 static int static_scratch_address(void** out) {
-  int dev = 0;
-  ZKB_TRY(check_cuda(cudaGetDevice(&dev), "cudaGetDevice"));
-  if (dev < 0 || dev >= 64) return fail(ZKB_EINVAL, "device index %d out of range", dev);
-  std::lock_guard<std::mutex> lock(g_static_scratch_mutex);
-  if (!g_static_scratch_addr[dev]) {
-    void* ptr = nullptr;
-    ZKB_TRY(check_cuda(cudaGetSymbolAddress(&ptr, g_msm_static_scratch),
-                       "cudaGetSymbolAddress(static MSM scratch)"));
-    g_static_scratch_addr[dev] = ptr;
-  }
-  *out = g_static_scratch_addr[dev];
+  void* ptr = nullptr;
+  ZKB_TRY(check_cuda(cudaGetSymbolAddress(&ptr, g_msm_static_scratch),
+                     "cudaGetSymbolAddress(static MSM scratch)"));
+  if (!ptr) return fail(ZKB_ECUDA, "cudaGetSymbolAddress returned no address for the static MSM scratch");
+  *out = ptr;
   return ZKB_OK;
 }
 
@@ -1364,6 +1363,9 @@ int zkb_msm_no_alloc(const uint64_t* points, const uint64_t* scalars, int64_t n,
                 "MSM of %lld points at window %d needs %zu bytes of scratch; the library's fixed "
                 "scratch holds %zu bytes (use zkb_msm with a caller-provided workspace)",
                 (long long)n, w, p.total, kNoAllocScratchBytes);
+  }
+  if ((int64_t)p.E >= (1ll << 31)) {
+    return fail(ZKB_EINVAL, "%lld points at window %d exceed the sort's 2^31 pairs", (long long)n, w);
   }
   void* scratch = nullptr;
   ZKB_TRY(static_scratch_address(&scratch));

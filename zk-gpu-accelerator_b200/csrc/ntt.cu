@@ -551,7 +551,9 @@ __global__ void __launch_bounds__(kNttThreads, 1) k_ntt_pass(F f, NttPass a) {
 
 static constexpr int kMaxBatchPasses = 192;  // 64 transforms x 3 passes
 static constexpr int kBatchThreads = 256;
-static constexpr unsigned kBatchSpinLimit = 1u << 22;  // x >= 256 ns each
+// Default bound of a dependency wait ("ntt.batch_spin_limit"): 2^22 polls,
+// each after a >= 256 ns sleep, about a second.
+static constexpr unsigned kBatchSpinLimit = 1u << 22;
 
 struct NttBatchTable {
   int num_passes;
@@ -563,7 +565,8 @@ struct NttBatchTable {
 template <class F, bool kShared>
 __global__ void __launch_bounds__(kBatchThreads) k_ntt_batch(F f, const __grid_constant__ NttBatchTable T,
                                                              unsigned long long* next_tile,
-                                                             unsigned* done, int* status) {
+                                                             unsigned* done, int* status,
+                                                             unsigned spin_limit) {
   extern __shared__ uint4 smem_raw[];
   uint64_t* sm = reinterpret_cast<uint64_t*>(smem_raw);
   __shared__ long long s_tile;
@@ -585,7 +588,7 @@ __global__ void __launch_bounds__(kBatchThreads) k_ntt_batch(F f, const __grid_c
           const unsigned need = (unsigned)(T.tile_start[d + 1] - T.tile_start[d]);
           unsigned spins = 0;
           while (*(volatile unsigned*)(done + d) < need) {
-            if (++spins > kBatchSpinLimit) {
+            if (++spins > spin_limit) {
               atomicExch(status, ZKB_ETIMEOUT);
               go = 0;
               break;
@@ -1094,7 +1097,9 @@ static int run_ntt_batch(const F& f, const zkb_field* field, const zkb_ntt_job* 
     if (per_sm < 1) per_sm = 1;
     const int64_t grid = std::min<int64_t>(tiles, (int64_t)sms * per_sm);
     ProfSpan span("ntt_batch", s);
-    kern<<<(unsigned)grid, kBatchThreads, smem, s>>>(f, T, next_tile, done, status);
+    const int spin_knob = tune_get("ntt.batch_spin_limit");
+    const unsigned spin_limit = spin_knob > 0 ? (unsigned)spin_knob : kBatchSpinLimit;
+    kern<<<(unsigned)grid, kBatchThreads, smem, s>>>(f, T, next_tile, done, status, spin_limit);
     ZKB_TRY(check_launch("NTT batch launch"));
   }
   if (status_out) {

@@ -31,6 +31,7 @@ static Knob g_knobs[] = {
     {"ntt.threads", 0, 0, 512},              // threads per NTT CTA (64..512; 0 = by tile)
     {"ntt.call_products", 0, 0, 1},          // pass kernels call one shared product (1) or inline all (0)
     {"ntt.full_table_mb", 4096, 0, 65536},   // budget of expanded NTT tables (MiB; 0 = two-level only)
+    {"ntt.batch_spin_limit", 0, 0, 1 << 30},  // polls before a batch tile's dependency wait gives up (0 = 2^22)
     {"ntt64.first_col_log", -1, -1, 6},      // int64 NTT first pass: log2 of input words per row (-1 = by size)
     {"ntt64.first_max_k", 0, 0, 10},         // int64 NTT first pass: stages (4..10; 0 = by size)
     {"ntt64.col_log", 0, 0, 6},              // int64 NTT later passes: log2 of words per row (1..6; 0 = by size)

@@ -73,6 +73,19 @@ class ZkbNttJob(ctypes.Structure):
     ]
 
 
+class ZkbIntPeaks(ctypes.Structure):
+    """zkb_int_peaks from include/zkb200.h: measured integer issue rates of the device."""
+
+    _fields_ = [
+        ("madlo_per_clk_sm", ctypes.c_double), ("madlo_per_s", ctypes.c_double), ("madlo_mhz", ctypes.c_double),
+        ("madwide_per_clk_sm", ctypes.c_double), ("madwide_per_s", ctypes.c_double),
+        ("madwide_mhz", ctypes.c_double),
+        ("montmul_per_clk_sm", ctypes.c_double), ("montmul_per_s", ctypes.c_double),
+        ("montmul_mhz", ctypes.c_double),
+        ("sms", ctypes.c_int32), ("reserved", ctypes.c_int32),
+    ]
+
+
 _u64p = ctypes.c_void_p  # device pointers travel as plain addresses
 _i64 = ctypes.c_int64
 _vp = ctypes.c_void_p
@@ -127,6 +140,7 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "zkb_msm_fixed_batch_workspace_bytes": (ctypes.c_size_t, [_jobp, ctypes.c_int]),
     "zkb_msm_fixed_batch": (ctypes.c_int, [_jobp, ctypes.c_int, _vp, ctypes.c_size_t, _vp]),
     "zkb_launch_count": (ctypes.c_uint64, []),
+    "zkb_measure_int_peaks": (ctypes.c_int, [ctypes.POINTER(ZkbIntPeaks), _vp]),
     "zkb_tune_set": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int]),
     "zkb_tune_get": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)]),
     "zkb_tune_set_sized": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int]),
@@ -263,6 +277,16 @@ def profile_report() -> dict[str, tuple[int, float]]:
         name, count, ms = line.split()
         out[name] = (int(count), float(ms))
     return out
+
+
+def measure_int_peaks() -> dict[str, float]:
+    """Measured issue rates of the current device (zkb_measure_int_peaks) as a dict: per SM per
+    clock, per second over the GPU, and the SM clock implied, for mad.lo.u32, mad.wide.u32 and the
+    library's Montgomery product over BN254 Fq."""
+    require_cuda()
+    out = ZkbIntPeaks()
+    check(lib().zkb_measure_int_peaks(ctypes.byref(out), stream_ptr()), "zkb_measure_int_peaks")
+    return {name: getattr(out, name) for name, _ in ZkbIntPeaks._fields_ if name != "reserved"}
 
 
 def workspace(nbytes: int) -> Any:

@@ -5,10 +5,12 @@ Drop-in for the reference's ntt_gpu (zkgpu/ntt_gpu.py:86-155): same
 arguments, roots (g^((p-1)/n) for the smallest non-residue g, as
 zkgpu/ntt.py:98-124, so the transform equals the CPU NTT element for
 element), validation and exceptions; the result is a torch int64 CUDA
-tensor. libzkb200.so (csrc/field64.cu) runs it: a bit-reversed load into
-Montgomery form, the first 11 stages of every 2048-word tile in shared
-memory, the remaining stages one pass each, and the way out of Montgomery
-form with n^-1 for an inverse. There is no CPU fallback.
+tensor. libzkb200.so (csrc/field64.cu, zkb_ntt64) runs it as a radix-2 DIT
+on bit-reversed input in two to four passes over HBM: the first pass gathers
+the bit-reversed rows of a tile and runs its first stages in shared memory,
+each later pass runs the next stages on tiles of rows at stride 2^S (Shoup
+products with precomputed quotients, in plain form), and the last pass
+multiplies by n^-1 for an inverse. There is no CPU fallback.
 """
 
 from __future__ import annotations
