@@ -97,6 +97,12 @@ int zkb_field_from_mont(const zkb_field* f, const uint64_t* in, uint64_t* out, i
 /* Device workspace (bytes) zkb_ntt needs for a transform of n rows. */
 size_t zkb_ntt_workspace_bytes(int64_t n);
 
+/* Number of NTT pass tiles on the current device, since the library loaded,
+ * whose bounded wait for their TMA loads gave up (each such block stops early
+ * and that transform's output is incomplete); 0 in a healthy run. It has no
+ * counterpart in the reference. Synchronous; ~0 if the device cannot be read. */
+uint64_t zkb_ntt_wait_timeouts(void);
+
 /* Replaces Field256.ntt / _ntt_on_gpu (zkgpu/field256_gpu.py:347-387) and the
  * GPU coset form of Radix2Domain.coset_fft / coset_ifft (zkgpu/domain.py:122-135):
  *   forward:  out[k] = sum_j in[j] * g^j * w^(j k)
@@ -346,6 +352,8 @@ int zkb_msm_fixed_batch(const zkb_msm_job* jobs, int count, void* workspace, siz
  * pass shape and direction the boundary twiddles of a non-last pass, per
  * coset transform its n scale factors, each saving one product per row;
  * default 4096, 0 = none);
+ * "ntt.tma" (1: transforms of two or more passes run TMA-fed persistent pass
+ * kernels; 0: the per-thread gather form; the same rows either way);
  * "ntt.batch_spin_limit" (polls, each after a sleep of at least 256 ns, before
  * a tile of zkb_ntt_batch gives up waiting for the previous pass of its
  * transform and reports ZKB_ETIMEOUT through the status word; 0 = the default

@@ -264,6 +264,8 @@ def test_ntt_matches_c_oracle_between_fixture_sizes(log_n):
         {"ntt.cta_log_elems": 10, "ntt.threads": 512},
         {"ntt.full_table_mb": 0},  # two-level twiddle and coset tables only
         {"ntt.max_log_radix": 8, "ntt.full_table_mb": 1},  # expanded tables for the small sizes only
+        {"ntt.tma": 0},  # per-thread gathers instead of the TMA-fed persistent passes
+        {"ntt.tma": 0, "ntt.max_log_radix": 12},
     ],
 )
 def test_ntt_pass_plans_give_the_same_rows(knobs):
@@ -297,6 +299,34 @@ def test_ntt_pass_plans_give_the_same_rows(knobs):
         _native.tune_set("ntt.cta_log_elems", 0)
         _native.tune_set("ntt.threads", 0)
         _native.tune_set("ntt.full_table_mb", 4096)
+        _native.tune_set("ntt.tma", 1)
+
+
+@pytest.mark.parametrize("cta_log", [9, 10, 11, 12])
+def test_tma_passes_equal_gather_passes_at_every_size(cta_log):
+    """The TMA-fed persistent passes (decimation in frequency over natural-order tiles) give the
+    rows of the per-thread gather passes (decimation in time over bit-reversed gathers) for
+    every size 2^2..2^22, forward / inverse / coset, at every tile size (two buffers up to
+    2048-row tiles, one at 4096); no tile's TMA wait gives up."""
+    from zkgpu import _native
+
+    lib = _native.lib()
+    before = lib.zkb_ntt_wait_timeouts()
+    try:
+        _native.tune_set("ntt.cta_log_elems", cta_log)
+        for log_n in range(2, 23):
+            n = 1 << log_n
+            rows = BN254_FR.to_montgomery(wl.uniform_fr(300 + log_n, n))
+            for invert, coset in ((False, None), (True, None), (False, 5), (True, 7)):
+                _native.tune_set("ntt.tma", 1)
+                got = BN254_FR.ntt(rows, invert=invert, coset=coset)
+                _native.tune_set("ntt.tma", 0)
+                want = BN254_FR.ntt(rows, invert=invert, coset=coset)
+                assert bool((got == want).all()), (log_n, invert, coset)
+    finally:
+        _native.tune_set("ntt.tma", 1)
+        _native.tune_set("ntt.cta_log_elems", 0)
+    assert lib.zkb_ntt_wait_timeouts() == before == 0
 
 
 def test_ntt_2_24_config_size():

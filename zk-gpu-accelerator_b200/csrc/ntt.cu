@@ -26,6 +26,7 @@
 
 #include "field_host.h"
 #include "profile.h"
+#include "tma.cuh"
 
 namespace zkb {
 
@@ -535,6 +536,330 @@ __global__ void __launch_bounds__(kNttThreads, 1) k_ntt_pass(F f, NttPass a) {
 }
 
 // ---------------------------------------------------------------------------
+// The pass kernel fed by TMA (the default for transforms of two or more passes)
+// ---------------------------------------------------------------------------
+//
+// Persistent: each CTA takes tiles blockIdx.x, blockIdx.x + gridDim.x, ...
+// One thread issues the tile's tensor loads (cp.async.bulk.tensor) into a
+// shared-memory buffer and the copies complete on that buffer's mbarrier; with
+// two buffers the loads of the CTA's next tile run while this tile computes.
+// A tile is C columns of R rows in natural order, split into two planes of
+// 16-byte half-elements (the low and the high 16 bytes of each 32-byte row),
+// so that consecutive rows read by consecutive lanes fall into distinct banks.
+// Two box loads per plane cover it (the low halves at word 0, the high halves
+// at word 2 of each row: both innermost coordinates are multiples of 16 bytes).
+//
+// The butterflies run decimation in frequency (natural order in, bit-reversed
+// order out): radix-4 rounds from the largest span down, after a radix-2 stage
+// when log2 R is odd. The first round applies the coset pre-scale as it reads
+// its rows. The store phase reads position p and writes it as frequency
+// k = brev(p), with the pass twiddle or the final scaling, as ntt_tile does.
+//
+// Plane layouts, as the boxes land: a non-last pass holds element (c, j) at
+// index j C + c (a box row is C neighbouring columns), the last pass at
+// c R + j (a box row is R neighbouring rows of one column). Lanes walk the
+// index that is contiguous, so each warp's accesses to a plane are
+// consecutive 16-byte words wherever the butterfly span allows.
+
+static constexpr uint32_t kTmaWaitLimit = 1u << 24;  // polls before a tile wait gives up
+static constexpr int kTmaBoxRows = 256;              // a TMA box extent is at most 256
+
+// Tiles whose TMA wait gave up (each such CTA stops early: its outputs are incomplete).
+__device__ unsigned g_ntt_tma_timeouts = 0;
+
+struct TmaPass {
+  int64_t ntiles;
+  int nbuf;       // 2: the next tile's loads overlap this tile's work; 1: one buffer
+  int four_d;     // the tensor map has four dimensions (else three: a last pass of a two-pass plan)
+};
+
+template <class F>
+__device__ __forceinline__ void plane_load(uint32_t x[8], const uint4* lo, const uint4* hi, int i) {
+  const uint4 l = lo[i], h = hi[i];
+  x[0] = l.x; x[1] = l.y; x[2] = l.z; x[3] = l.w;
+  x[4] = h.x; x[5] = h.y; x[6] = h.z; x[7] = h.w;
+}
+
+__device__ __forceinline__ void plane_store(uint4* lo, uint4* hi, int i, const uint32_t x[8]) {
+  lo[i] = make_uint4(x[0], x[1], x[2], x[3]);
+  hi[i] = make_uint4(x[4], x[5], x[6], x[7]);
+}
+
+template <class F>
+__global__ void __launch_bounds__(kNttThreads) k_ntt_pass_tma(F f, const NttPass a, const TmaPass tp,
+                                                             const __grid_constant__ CUtensorMap tmap) {
+  extern __shared__ __align__(1024) unsigned char smem_raw_tma[];
+  // the buffers start on a 1 KiB boundary (the launch asks for 1 KiB more)
+  unsigned char* smem_tma = smem_raw_tma + ((1024u - (smem_u32(smem_raw_tma) & 1023u)) & 1023u);
+  const int lr = a.lr, lc = a.lc;
+  const int R = 1 << lr, C = 1 << lc, T = C << lr;
+  const int64_t S = 1ll << a.ls;
+  const int64_t B = (int64_t)R << a.ls;
+  const int nbuf = tp.nbuf;
+  const size_t plane = (size_t)T * 16;
+  unsigned char* bufs = smem_tma;
+  uint64_t* tw = reinterpret_cast<uint64_t*>(smem_tma + (size_t)nbuf * 2 * plane);
+  uint64_t* bars = tw + 4 * (R >> 1);
+  const int tid = threadIdx.x;
+
+  for (int j = tid; j < (R >> 1); j += blockDim.x) {
+    uint32_t w[8];
+    fe_load_nc(w, a.w + 4 * ((int64_t)j << (a.log_rmax - lr)));
+    fe_store(tw + 4 * j, w);
+  }
+  if (tid == 0) {
+    for (int b = 0; b < nbuf; ++b) mbar_init(&bars[b], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+
+  const int rows_box = R < kTmaBoxRows ? R : kTmaBoxRows;
+  const int64_t groups = S >> lc;  // non-last pass: tiles per block of B rows
+  // thread 0: announce the tile's bytes and issue its box loads into buffer b
+  auto issue = [&](int64_t tile, int b) {
+    unsigned char* lo = bufs + (size_t)b * 2 * plane;
+    unsigned char* hi = lo + plane;
+    mbar_arrive_expect_tx(&bars[b], (uint32_t)T * 32u);
+    if (!a.last) {
+      const int o = (int)(tile / groups);
+      const int j0 = (int)((tile % groups) << lc);
+      for (int r0 = 0; r0 < R; r0 += rows_box) {
+        const size_t off = (size_t)r0 * C * 16;
+        tma_load_4d(lo + off, &tmap, &bars[b], 0, j0, r0, o);
+        tma_load_4d(hi + off, &tmap, &bars[b], 2, j0, r0, o);
+      }
+    } else {
+      // a box holds all C columns when a column fits one box (R <= 256), else one
+      // column's run of rows_box rows; either way column c lands at c R
+      const int k2 = (int)(tile & ((1ll << a.lR2) - 1));
+      const int k1_0 = (int)((tile >> a.lR2) << lc);
+      const int box_cols = R <= kTmaBoxRows ? C : 1;
+      for (int c0 = 0; c0 < C; c0 += box_cols) {
+        for (int r0 = 0; r0 < R; r0 += rows_box) {
+          const size_t off = ((size_t)c0 * R + r0) * 16;
+          if (tp.four_d) {
+            tma_load_4d(lo + off, &tmap, &bars[b], 0, r0, k2, k1_0 + c0);
+            tma_load_4d(hi + off, &tmap, &bars[b], 2, r0, k2, k1_0 + c0);
+          } else {
+            tma_load_3d(lo + off, &tmap, &bars[b], 0, r0, k1_0 + c0);
+            tma_load_3d(hi + off, &tmap, &bars[b], 2, r0, k1_0 + c0);
+          }
+        }
+      }
+    }
+  };
+  // plane index of element (c, j)
+  auto pidx = [&](int c, int j) { return a.last ? (c << lr) + j : (j << lc) + c; };
+
+  int64_t tile = blockIdx.x;
+  if (tid == 0 && tile < tp.ntiles) issue(tile, 0);
+  bool failed = false;
+  int64_t i = 0;
+  for (; tile < tp.ntiles; ++i, tile += gridDim.x) {
+    const int b = nbuf == 2 ? (int)(i & 1) : 0;
+    const uint32_t parity = nbuf == 2 ? (uint32_t)((i >> 1) & 1) : (uint32_t)(i & 1);
+    if (nbuf == 2 && tid == 0 && tile + gridDim.x < tp.ntiles) issue(tile + gridDim.x, b ^ 1);
+    const bool got = mbar_wait_bounded(&bars[b], parity, kTmaWaitLimit);
+    if (__syncthreads_or(!got)) {
+      failed = true;
+      break;
+    }
+    uint4* lo = reinterpret_cast<uint4*>(bufs + (size_t)b * 2 * plane);
+    uint4* hi = reinterpret_cast<uint4*>(bufs + (size_t)b * 2 * plane + plane);
+
+    // tile origin in the pass's index space
+    int64_t o = 0, j0 = 0, k2 = 0, k1_0 = 0;
+    if (!a.last) {
+      o = tile / groups;
+      j0 = (tile % groups) << lc;
+    } else {
+      k2 = tile & ((1ll << a.lR2) - 1);
+      k1_0 = (tile >> a.lR2) << lc;
+    }
+    const bool prescale = a.first && a.g_lo && !a.inverse;
+    // the coset factor g^pos of element (c, j): only the first pass, which is never the last
+    auto scale_in = [&](uint32_t x[8], int c, int j) {
+      const int64_t pos = o * B + (int64_t)j * S + j0 + c;
+      uint32_t g[8];
+      if (a.g_full) {
+        fe_load_nc(g, a.g_full + 4 * pos);
+      } else {
+        const uint64_t m = (1ull << a.gs) - 1;
+        uint32_t hi2[8];
+        fe_load_nc(g, a.g_lo + 4 * ((uint64_t)pos & m));
+        fe_load_nc(hi2, a.g_hi + 4 * ((uint64_t)pos >> a.gs));
+        fe_mul(g, g, hi2, f);
+      }
+      fe_mul(x, x, g, f);
+    };
+
+    // ---- decimation in frequency ----
+    bool first_round = true;
+    int st = lr - 1;
+    if (lr & 1) {  // radix-2 stage of half-span R / 2
+      const int h = 1 << st;
+      for (int u = tid; u < (T >> 1); u += blockDim.x) {
+        int c, q;
+        if (!a.last) {
+          c = u & (C - 1);
+          q = u >> lc;
+        } else {
+          q = u & (h - 1);
+          c = u >> (lr - 1);
+        }
+        uint32_t x0[8], x1[8], t[8];
+        const int i0 = pidx(c, q), i1 = pidx(c, q + h);
+        plane_load<F>(x0, lo, hi, i0);
+        plane_load<F>(x1, lo, hi, i1);
+        if (prescale) {
+          scale_in(x0, c, q);
+          scale_in(x1, c, q + h);
+        }
+        fe_add(t, x0, x1, f);
+        fe_sub(x1, x0, x1, f);
+        if (st > 0) {
+          uint32_t w[8];
+          fe_load(w, tw + 4 * q);  // w_R^q
+          fe_mul(x1, x1, w, f);
+        }
+        plane_store(lo, hi, i0, t);
+        plane_store(lo, hi, i1, x1);
+      }
+      first_round = false;
+      __syncthreads();
+      st -= 1;
+    }
+    // radix-4 rounds: st is the lower stage of the pair (half-spans 2h and h)
+    for (st -= 1; st >= 0; st -= 2) {
+      const int h = 1 << st;
+      const int R4 = R >> 2;
+      for (int u = tid; u < (T >> 2); u += blockDim.x) {
+        int c, q;
+        if (!a.last) {
+          c = u & (C - 1);
+          q = u >> lc;
+        } else {
+          q = u & (R4 - 1);
+          c = u >> (lr - 2);
+        }
+        const int jj = q & (h - 1);
+        const int i0 = ((q >> st) << (st + 2)) | jj;
+        uint32_t x0[8], x1[8], x2[8], x3[8], t[8], w[8];
+        plane_load<F>(x0, lo, hi, pidx(c, i0));
+        plane_load<F>(x1, lo, hi, pidx(c, i0 + h));
+        plane_load<F>(x2, lo, hi, pidx(c, i0 + 2 * h));
+        plane_load<F>(x3, lo, hi, pidx(c, i0 + 3 * h));
+        if (prescale && first_round) {
+          scale_in(x0, c, i0);
+          scale_in(x1, c, i0 + h);
+          scale_in(x2, c, i0 + 2 * h);
+          scale_in(x3, c, i0 + 3 * h);
+        }
+        // half-span 2h: (x0, x2) with w_4h^jj, (x1, x3) with w_4h^(jj + h)
+        fe_add(t, x0, x2, f);
+        fe_sub(x2, x0, x2, f);
+        fe_copy(x0, t);
+        fe_add(t, x1, x3, f);
+        fe_sub(x3, x1, x3, f);
+        fe_copy(x1, t);
+        if (st > 0) {
+          fe_load(w, tw + 4 * (jj << (lr - 2 - st)));
+          fe_mul(x2, x2, w, f);
+        }
+        fe_load(w, tw + 4 * ((jj + h) << (lr - 2 - st)));
+        fe_mul(x3, x3, w, f);
+        // half-span h: (x0, x1) and (x2, x3) with w_2h^jj
+        fe_add(t, x0, x1, f);
+        fe_sub(x1, x0, x1, f);
+        fe_copy(x0, t);
+        fe_add(t, x2, x3, f);
+        fe_sub(x3, x2, x3, f);
+        fe_copy(x2, t);
+        if (st > 0) {
+          fe_load(w, tw + 4 * (jj << (lr - 1 - st)));
+          fe_mul(x1, x1, w, f);
+          fe_mul(x3, x3, w, f);
+        }
+        plane_store(lo, hi, pidx(c, i0), x0);
+        plane_store(lo, hi, pidx(c, i0 + h), x1);
+        plane_store(lo, hi, pidx(c, i0 + 2 * h), x2);
+        plane_store(lo, hi, pidx(c, i0 + 3 * h), x3);
+      }
+      first_round = false;
+      __syncthreads();
+    }
+
+    // ---- store: position p holds frequency k = brev(p) ----
+    for (int t = tid; t < T; t += blockDim.x) {
+      int c, p;
+      if (!a.last) {
+        c = t & (C - 1);
+        p = t >> lc;
+      } else {
+        p = t & (R - 1);
+        c = t >> lr;
+      }
+      const int k = lr ? (int)(__brev((unsigned)p) >> (32 - lr)) : 0;
+      uint32_t x[8];
+      plane_load<F>(x, lo, hi, pidx(c, p));
+      if (!a.last) {
+        const int64_t jp = j0 + c;
+        uint64_t e = ((uint64_t)(jp * k)) << (a.log_N - (lr + a.ls));
+        if (a.inverse && e) e = (1ull << a.log_N) - e;
+        if (e) {
+          uint32_t w[8];
+          if (a.t_full) {
+            fe_load_nc(w, a.t_full + 4 * (((int64_t)k << a.ls) + jp));
+          } else {
+            root_power<false>(w, a, e, f);
+          }
+          fe_mul(x, x, w, f);
+        }
+        fe_store(a.out + 4 * (o * B + (int64_t)k * S + jp), x);
+      } else {
+        const int64_t oc = ((k1_0 + c) << a.lR2) + k2;
+        const int64_t outidx = (oc >> a.lR2) + ((oc & ((1ll << a.lR2) - 1)) << a.lR1) +
+                               ((int64_t)k << (a.log_n - lr));
+        if (a.inverse) {
+          uint32_t sc[8];
+          if (a.g_full) {
+            fe_load_nc(sc, a.g_full + 4 * outidx);
+          } else if (a.g_lo) {
+            const uint64_t m = (1ull << a.gs) - 1;
+            uint32_t l2[8], h2[8];
+            fe_load_nc(l2, a.g_lo + 4 * ((uint64_t)outidx & m));
+            fe_load_nc(h2, a.g_hi + 4 * ((uint64_t)outidx >> a.gs));
+            fe_mul(sc, l2, h2, f);
+          } else {
+            fe_load_nc(sc, a.scale);
+          }
+          fe_mul(x, x, sc, f);
+        }
+        fe_store(a.out + 4 * outidx, x);
+      }
+    }
+    // every thread is done with this buffer (generic accesses) before the next
+    // TMA write into it
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (nbuf == 1 && tid == 0 && tile + gridDim.x < tp.ntiles) issue(tile + gridDim.x, 0);
+  }
+  if (failed) {
+    // a wait gave up: record it, and let the copies still in flight land (bounded)
+    // before the CTA's shared memory goes away
+    if (tid == 0) {
+      atomicAdd(&g_ntt_tma_timeouts, 1u);
+      const int b = nbuf == 2 ? (int)(i & 1) : 0;
+      mbar_wait_bounded(&bars[b], nbuf == 2 ? (uint32_t)((i >> 1) & 1) : (uint32_t)(i & 1), kTmaWaitLimit);
+      if (nbuf == 2 && tile + gridDim.x < tp.ntiles) {
+        mbar_wait_bounded(&bars[b ^ 1], (uint32_t)(((i + 1) >> 1) & 1), kTmaWaitLimit);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Batched form: one persistent launch for many transforms
 // ---------------------------------------------------------------------------
 //
@@ -937,6 +1262,60 @@ static int sm_count(int device, int* sms) {
                     "SM count");
 }
 
+// One pass through k_ntt_pass_tma: its tensor map over the pass's input, the
+// shared-memory plan (two tile buffers when four planes fit in about 110 KiB,
+// else one) and a one-wave persistent grid.
+template <class F>
+static int launch_pass_tma(const F& f, const PassLaunch& L, int64_t n, int P, int sms, cudaStream_t s, int q) {
+  const NttPass& a = L.a;
+  const int R = 1 << a.lr, C = 1 << a.lc;
+  const int64_t T = (int64_t)C << a.lr;
+  const uint32_t rows_box = (uint32_t)std::min(R, kTmaBoxRows);
+  CUtensorMap map;
+  TmaPass tp;
+  tp.ntiles = n / T;
+  if (!a.last) {
+    const uint64_t S = 1ull << a.ls, B = (uint64_t)R << a.ls;
+    const uint64_t dims[4] = {4, S, (uint64_t)R, (uint64_t)n / B};
+    const uint64_t strides[3] = {32, S * 32, B * 32};
+    const uint32_t box[4] = {2, (uint32_t)C, rows_box, 1};
+    ZKB_TRY(encode_tensor_map_u64(&map, a.in, 4, dims, strides, box));
+    tp.four_d = 1;
+  } else if (a.lR2 > 0) {
+    const uint64_t R1 = 1ull << a.lR1, R2 = 1ull << a.lR2;
+    const uint32_t box_cols = R <= kTmaBoxRows ? (uint32_t)C : 1u;  // as the kernel's issue loop
+    const uint64_t dims[4] = {4, (uint64_t)R, R2, R1};
+    const uint64_t strides[3] = {32, (uint64_t)R * 32, R2 * R * 32};
+    const uint32_t box[4] = {2, rows_box, 1, box_cols};
+    ZKB_TRY(encode_tensor_map_u64(&map, a.in, 4, dims, strides, box));
+    tp.four_d = 1;
+  } else {
+    const uint64_t R1 = 1ull << a.lR1;
+    const uint32_t box_cols = R <= kTmaBoxRows ? (uint32_t)C : 1u;
+    const uint64_t dims[3] = {4, (uint64_t)R, R1};
+    const uint64_t strides[2] = {32, (uint64_t)R * 32};
+    const uint32_t box[3] = {2, rows_box, box_cols};
+    ZKB_TRY(encode_tensor_map_u64(&map, a.in, 3, dims, strides, box));
+    tp.four_d = 0;
+  }
+  const size_t plane = (size_t)T * 16;
+  const size_t rest = ((size_t)R >> 1) * 32 + 2 * 8 + 1024;  // stage table, barriers, alignment slack
+  tp.nbuf = 4 * plane + rest <= (110u << 10) ? 2 : 1;
+  const size_t smem = (size_t)tp.nbuf * 2 * plane + rest;
+  auto kern = k_ntt_pass_tma<F>;
+  ZKB_TRY(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                     "NTT pass shared memory attribute"));
+  int per_sm = 0;
+  ZKB_TRY(check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, L.threads, smem),
+                     "NTT pass occupancy"));
+  if (per_sm < 1) return fail(ZKB_ECUDA, "NTT pass of %d threads and %zu bytes does not fit an SM", L.threads, smem);
+  const int64_t grid = std::min<int64_t>(tp.ntiles, (int64_t)sms * per_sm);
+  ProfSpan span(a.last ? "ntt_last_pass" : "ntt_column_pass", s);
+  (void)q;
+  kern<<<(unsigned)grid, L.threads, smem, s>>>(f, a, tp, map);
+  return check_launch("NTT pass launch (TMA)");
+}
+
 template <class F>
 static int run_ntt(const F& f, const zkb_field* field, const uint64_t* in, uint64_t* out,
                    int64_t n, int invert, const uint64_t* omega, const uint64_t* coset,
@@ -959,11 +1338,18 @@ static int run_ntt(const F& f, const zkb_field* field, const uint64_t* in, uint6
   plan_passes(n, log_n, invert, rt, st, in, out, reinterpret_cast<uint64_t*>(workspace), 0, 0,
               false, passes);
   const int P = (int)passes.size();
+  const bool tma = P >= 2 && tune_get("ntt.tma") != 0;
+  int sms = 0;
+  if (tma) ZKB_TRY(sm_count(device, &sms));
   for (int q = 0; q < P; ++q) {
     if (!passes[q].a.last) {
       ZKB_TRY(lookup_twiddles(f, key, rt, passes[q].a.lr, passes[q].a.ls, invert, &passes[q].a.t_full, s));
     }
     const PassLaunch& L = passes[q];
+    if (tma) {
+      ZKB_TRY(launch_pass_tma(f, L, n, P, sms, s, q));
+      continue;
+    }
     auto kern = tune_get("ntt.call_products") ? k_ntt_pass<F, true> : k_ntt_pass<F, false>;
     ZKB_TRY(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)L.smem),
@@ -1238,6 +1624,12 @@ using namespace zkb;
 extern "C" {
 
 size_t zkb_ntt_workspace_bytes(int64_t n) { return zkb::workspace_bytes(n); }
+
+uint64_t zkb_ntt_wait_timeouts(void) {
+  unsigned v = 0;
+  if (cudaMemcpyFromSymbol(&v, zkb::g_ntt_tma_timeouts, sizeof v) != cudaSuccess) return ~0ull;
+  return v;
+}
 
 int zkb_ntt(const zkb_field* f, const uint64_t* in, uint64_t* out, int64_t n, int invert,
             const uint64_t* omega, const uint64_t* coset, void* workspace,

@@ -5,6 +5,7 @@
 
 #include "common.cuh"
 #include "field_host.h"
+#include "tma.cuh"
 
 namespace zkb {
 
@@ -32,6 +33,7 @@ static Knob g_knobs[] = {
     {"ntt.call_products", 0, 0, 1},          // pass kernels call one shared product (1) or inline all (0)
     {"ntt.full_table_mb", 4096, 0, 65536},   // budget of expanded NTT tables (MiB; 0 = two-level only)
     {"ntt.batch_spin_limit", 0, 0, 1 << 30},  // polls before a batch tile's dependency wait gives up (0 = 2^22)
+    {"ntt.tma", 1, 0, 1},                    // multi-pass transforms: TMA-fed persistent passes (1) or per-thread gathers (0)
     {"ntt64.first_col_log", -1, -1, 6},      // int64 NTT first pass: log2 of input words per row (-1 = by size)
     {"ntt64.first_max_k", 0, 0, 10},         // int64 NTT first pass: stages (4..10; 0 = by size)
     {"ntt64.col_log", 0, 0, 6},              // int64 NTT later passes: log2 of words per row (1..6; 0 = by size)
@@ -172,6 +174,55 @@ int check_field(const zkb_field* f) {
   if (f->kind != ZKB_FIELD_GENERIC && f->kind != ZKB_FIELD_BN254_FR && f->kind != ZKB_FIELD_BN254_FQ) {
     return fail(ZKB_EINVAL, "field not initialised by zkb_field_init");
   }
+  return ZKB_OK;
+}
+
+// ---- tensor maps --------------------------------------------------------------
+// cuTensorMapEncodeTiled is a driver entry point; the runtime hands out its
+// address, so the library needs no link against the driver library.
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_tiled_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess) {
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+  });
+  return fn;
+}
+
+int encode_tensor_map_u64(CUtensorMap* map, const void* base, int rank, const uint64_t* dims,
+                          const uint64_t* strides_bytes, const uint32_t* box) {
+  EncodeTiledFn fn = encode_tiled_fn();
+  if (!fn) return fail(ZKB_ECUDA, "cuTensorMapEncodeTiled is not available from the driver");
+  if (rank < 2 || rank > 5) return fail(ZKB_EINVAL, "tensor map rank %d out of 2..5", rank);
+  if (reinterpret_cast<uintptr_t>(base) & 15) return fail(ZKB_EINVAL, "tensor map base must be 16-byte aligned");
+  cuuint64_t gdim[5], gstride[4];
+  cuuint32_t bdim[5], estride[5];
+  for (int i = 0; i < rank; ++i) {
+    gdim[i] = dims[i];
+    bdim[i] = box[i];
+    estride[i] = 1;
+    if (box[i] < 1 || box[i] > 256 || box[i] > dims[i]) {
+      return fail(ZKB_EINVAL, "tensor map box dimension %d (%u) out of range", i, box[i]);
+    }
+  }
+  if ((box[0] * 8u) % 16u) return fail(ZKB_EINVAL, "tensor map box inner extent must be a multiple of 16 bytes");
+  for (int i = 0; i + 1 < rank; ++i) {
+    gstride[i] = strides_bytes[i];
+    if (strides_bytes[i] % 16) return fail(ZKB_EINVAL, "tensor map stride %d not a multiple of 16 bytes", i);
+  }
+  const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT64, (cuuint32_t)rank, const_cast<void*>(base), gdim,
+                        gstride, bdim, estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(ZKB_ECUDA, "cuTensorMapEncodeTiled failed (CUresult %d)", (int)r);
   return ZKB_OK;
 }
 

@@ -104,6 +104,7 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "zkb_field_to_mont": (ctypes.c_int, [_fp, _u64p, _u64p, _i64, _vp]),
     "zkb_field_from_mont": (ctypes.c_int, [_fp, _u64p, _u64p, _i64, _vp]),
     "zkb_ntt_workspace_bytes": (ctypes.c_size_t, [_i64]),
+    "zkb_ntt_wait_timeouts": (ctypes.c_uint64, []),
     "zkb_ntt": (
         ctypes.c_int,
         [_fp, _u64p, _u64p, _i64, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64),
