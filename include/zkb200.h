@@ -352,8 +352,15 @@ int zkb_msm_fixed_batch(const zkb_msm_job* jobs, int count, void* workspace, siz
  * pass shape and direction the boundary twiddles of a non-last pass, per
  * coset transform its n scale factors, each saving one product per row;
  * default 4096, 0 = none);
- * "ntt.tma" (1: transforms of two or more passes run TMA-fed persistent pass
- * kernels; 0: the per-thread gather form; the same rows either way);
+ * "ntt.tma" (1: transforms of two or more passes run TMA-fed pass kernels;
+ * 0: the per-thread gather form; the same rows either way), "ntt.tma_grid"
+ * (1: one tile per block; 0: one persistent wave of double-buffered blocks),
+ * "ntt.tma_blocks_per_sm" (0, or 5 / 6: the pass kernel of 128-thread blocks
+ * with its registers capped for that many blocks per SM);
+ * "msm.affine_rounds" (rounds in which every bucket's list is halved by affine
+ * additions sharing one inversion per block, before the XYZZ levels; 0 = none,
+ * the default; -1 = by size; 1..8 forced), "msm.affine_batch" (output entries
+ * per thread of such a round, 8..512; default 64);
  * "ntt.batch_spin_limit" (polls, each after a sleep of at least 256 ns, before
  * a tile of zkb_ntt_batch gives up waiting for the previous pass of its
  * transform and reports ZKB_ETIMEOUT through the status word; 0 = the default

@@ -223,3 +223,89 @@ def test_workspace_too_small_is_an_error():
     assert status == _native.ZKB_EWORKSPACE
     assert "workspace" in _native.last_error()
     assert ctypes.c_int(status).value == 5
+
+
+# ------------------------------------------------------------------
+# Affine rounds (batch-affine bucket additions before the XYZZ levels)
+# ------------------------------------------------------------------
+
+
+def _with_knobs(knobs: dict, fn):
+    old = {k: _native.tune_get(k) for k in knobs}
+    try:
+        for k, v in knobs.items():
+            _native.tune_set(k, v)
+        return fn()
+    finally:
+        for k, v in old.items():
+            _native.tune_set(k, v)
+
+
+@pytest.mark.parametrize("rounds", [1, 2, 3, 6])
+@pytest.mark.parametrize("batch", [8, 64])
+@pytest.mark.parametrize("case", golden("msm.json")["seeded"], ids=lambda c: f"{c['kind']}-{c['n']}")
+def test_affine_rounds_give_the_references_points(case, rounds, batch):
+    """Forced affine rounds (each bucket list halved by affine additions with one inversion per
+    block) at the seeded sizes, uniform and skewed, against the reference's points."""
+    n = case["n"]
+    bases = _bases(n, case["base_seed"])
+    gen = wl.uniform_fr if case["kind"] == "uniform" else wl.skewed_scalars
+    sc = gen(case["scalar_seed"], n)
+    knobs = {"msm.affine_rounds": rounds, "msm.affine_batch": batch}
+    for w in (None, 6, 13):
+        assert _with_knobs(knobs, lambda: msm_pippenger_rows(bases, sc, window_size=w)) == expected_point(case), w
+
+
+@pytest.mark.parametrize("rounds", [1, 2, 4])
+def test_affine_rounds_special_cases(rounds):
+    """Buckets whose pairs hit every case of the affine addition: P + P (a doubling),
+    P + (-P) (infinity, which later rounds and the XYZZ levels must skip), infinity + Q and
+    Q + infinity (copies), and odd list lengths; against double-and-add on the CPU."""
+    k = [1, 2, 3, 5, 8]
+    base = [po.scalar_mul(po.G, v) for v in k]
+    neg = [(x, (P - y) % P) for x, y in base]
+    pts = []
+    for i in range(40):  # runs of equal points, their negatives, and mixtures
+        pts += [base[i % 5]] * (1 + i % 3) + [neg[i % 5]] * (i % 2) + [base[(i + 1) % 5]]
+    scalars_list = [[1] * len(pts), [2**64 + 3] * len(pts), [(i % 7) + 1 for i in range(len(pts))]]
+    xs, ys = [p[0] for p in pts], [p[1] for p in pts]
+    for scalars in scalars_list:
+        want = po.msm_double_and_add(pts, scalars)
+        want = Point.identity() if want is None else Point(*want)
+        got = _with_knobs({"msm.affine_rounds": rounds, "msm.affine_batch": 8},
+                          lambda: msm_pippenger_gpu(xs, ys, scalars, window_size=4))
+        assert got == want
+    # a bucket that sums to exactly infinity: P, -P, 2P, -2P, all with one scalar
+    two = po.scalar_mul(po.G, 2)
+    cancel = [base[0], neg[0], two, (two[0], (P - two[1]) % P)]
+    got = _with_knobs({"msm.affine_rounds": rounds, "msm.affine_batch": 8},
+                      lambda: msm_pippenger_gpu([p[0] for p in cancel], [p[1] for p in cancel], [9] * 4))
+    assert got == Point.identity()
+
+
+def test_affine_rounds_in_batches_and_fixed_base_tables():
+    """Batched MSMs (one pipeline for several jobs) and MSMs over a fixed-base table with
+    forced affine rounds give the points of the plain path."""
+    from zkgpu import batch
+    from zkgpu.msm_gpu import FixedBaseTable
+
+    n = 1 << 14
+    bases = _bases(n, 77)
+    scs = [wl.uniform_fr(78, n), wl.skewed_scalars(79, n // 2), wl.uniform_fr(80, 1000)]
+    pts = [bases, bases[: n // 2], bases[:1000]]
+    want = [msm_pippenger_rows(p, s) for p, s in zip(pts, scs)]
+    knobs = {"msm.affine_rounds": 3, "msm.affine_batch": 16}
+    assert _with_knobs(knobs, lambda: batch.msm_batch(pts, scs)) == want
+    table = FixedBaseTable(bases, 12)
+    got = _with_knobs(knobs, lambda: batch.msm_fixed_batch(table, scs[:2]))
+    assert got == want[:2]
+
+
+def test_affine_rounds_with_inlined_products():
+    case = golden("msm.json")["seeded"][0]
+    n = case["n"]
+    bases = _bases(n, case["base_seed"])
+    gen = wl.uniform_fr if case["kind"] == "uniform" else wl.skewed_scalars
+    sc = gen(case["scalar_seed"], n)
+    knobs = {"msm.affine_rounds": 2, "msm.affine_batch": 32, "msm.call_products": 0}
+    assert _with_knobs(knobs, lambda: msm_pippenger_rows(bases, sc)) == expected_point(case)

@@ -473,6 +473,10 @@ __device__ __forceinline__ void xyzz_add(Xyzz& r, const Xyzz& p, const Xyzz& q) 
   fe_copy(r.zzz, zzz);
 }
 
+// The MSM's affine bucket lists mark the point at infinity by bit 255 of x,
+// which a canonical coordinate (below q < 2^254) never sets.
+__device__ __forceinline__ bool aff_is_inf(const Aff& p) { return (p.x[7] >> 31) != 0; }
+
 // Negate an affine point: (x, -y).
 __device__ __forceinline__ void aff_neg(Aff& q) {
   G1F f;

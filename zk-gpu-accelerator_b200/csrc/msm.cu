@@ -565,6 +565,7 @@ __device__ __forceinline__ void acc_points(const MsmJobs& J, const uint32_t* key
     const int64_t idx = (int64_t)(v & 0x7fffffffu);
     Aff q;
     aff_load_nc(q, idx < jp.n ? jp.points + 8 * idx : jp.phi + 8 * (idx - jp.n));
+    if (aff_is_inf(q)) continue;  // a bucket entry that summed to infinity in an affine round
     if (v >> 31) aff_neg(q);
     xyzz_add_affine<M>(acc, q);
   }
@@ -592,6 +593,356 @@ __global__ void __launch_bounds__(128, 4) k_msm_acc_points_batch(const MsmJobs J
                                                                  uint32_t* slot_keys,
                                                                  uint64_t* slot_pts) {
   acc_points<true, M>(J, keys, vals, st, E, E_dev, K, none, buckets, slot_keys, slot_pts);
+}
+
+// ---------------------------------------------------------------------------
+// 3a. affine rounds before the XYZZ levels (large MSMs)
+// ---------------------------------------------------------------------------
+//
+// Each round halves every bucket's list: entry m of a bucket's output is the
+// sum of its input entries 2m and 2m + 1 (or a copy of entry 2m when it is the
+// last), added in affine coordinates. An affine addition needs the inverse of
+// x2 - x1; with the inverses shared (Montgomery's simultaneous inversion) it
+// costs 5 products and 1 squaring, against 8 and 2 for the XYZZ mixed
+// addition the run kernels use. Round 0 reads the sorted pairs and gathers the
+// points (signs applied); later rounds read the previous round's points. The
+// bucket layout of a round is its list of bucket ends (an inclusive scan of
+// the halved counts). After the last round, the short lists go through the
+// XYZZ run and merge levels as (bucket, entry) pairs.
+//
+// The sharing is per block and pipelined. Warps 0..6 are workers: in a batch
+// each worker thread chains the denominators of its k output entries into one
+// running product, and the workers' products are combined by prefix and
+// suffix products across lanes (shuffles) and across warps. Warp 7 inverts the
+// batch's product (one exponentiation, a few hundred dependent products) while
+// the workers walk the previous batch's chains back with the inverse it
+// produced one iteration earlier; so the exponentiation's latency overlaps the
+// additions instead of stalling them. Blocks are persistent: block b takes
+// batches b, b + gridDim.x, ... of 224 k output entries.
+//
+// Special cases, decided when the denominator is formed (the case travels to
+// the backward walk in `meta`): equal x and equal y is a doubling (the
+// denominator is 2y); equal x otherwise (P + (-P)) gives the point at infinity;
+// an operand at infinity (bit 255 of x set) makes the result the other
+// operand. Those cases put 1 into the chain, so no zero reaches an inversion.
+
+static constexpr int kAffThreads = 256;
+static constexpr int kAffWorkerWarps = 7;
+static constexpr int kAffWorkers = kAffWorkerWarps * 32;
+static constexpr uint32_t kAffAdd = 0, kAffDbl = 1, kAffInf = 2, kAffCopy1 = 3, kAffCopy2 = 4;
+
+__device__ __forceinline__ void aff_store_inf(uint64_t* dst) {
+  uint32_t z[8];
+  fe_zero(z);
+  fe_store(dst + 4, z);
+  z[7] = 0x80000000u;
+  fe_store(dst, z);
+}
+
+// half[b] = ceil(n_b / 2), n_b = ends[b] - ends[b - 1] (ends[-1] = 0).
+__global__ void __launch_bounds__(256) k_msm_half_counts(const uint32_t* ends, int keys, uint32_t* half) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < keys; b += stride) {
+    const uint32_t n = ends[b] - (b ? ends[b - 1] : 0u);
+    half[b] = (n + 1u) >> 1;
+  }
+}
+
+// The bucket holding output entry e: the first b with ends[b] > e.
+__device__ __forceinline__ int bucket_of_entry(const uint32_t* ends, int keys, uint32_t e) {
+  int lo = 0, hi = keys - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (ends[mid] > e) hi = mid; else lo = mid + 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ void shfl_up8(uint32_t r[8], const uint32_t a[8], int o) {
+#pragma unroll
+  for (int j = 0; j < 8; ++j) r[j] = __shfl_up_sync(0xffffffffu, a[j], o);
+}
+__device__ __forceinline__ void shfl_down8(uint32_t r[8], const uint32_t a[8], int o) {
+#pragma unroll
+  for (int j = 0; j < 8; ++j) r[j] = __shfl_down_sync(0xffffffffu, a[j], o);
+}
+
+// Exclusive prefix and suffix products of v across the warp's lanes (1 at the ends).
+template <class M>
+__device__ __forceinline__ void warp_exclusive_products(uint32_t xp[8], uint32_t xs[8], const uint32_t v[8],
+                                                        int lane) {
+  G1F f;
+  uint32_t pre[8], suf[8], t[8];
+  fe_copy(pre, v);
+  fe_copy(suf, v);
+#pragma unroll 1
+  for (int o = 1; o < 32; o <<= 1) {
+    shfl_up8(t, pre, o);
+    if (lane >= o) M::mul(pre, pre, t);
+    shfl_down8(t, suf, o);
+    if (lane + o < 32) M::mul(suf, suf, t);
+  }
+  shfl_up8(xp, pre, 1);
+  shfl_down8(xs, suf, 1);
+  if (lane == 0) fe_one(xp, f);
+  if (lane == 31) fe_one(xs, f);
+}
+
+// An entry's two source rows, as the forward walk resolves them and the
+// backward walk reads them back from `meta`: the row addresses with the sign
+// of the y coordinate in bit 0 (rows are 64-byte aligned) and the entry's case
+// in bits 1..3 of the first.
+struct AffMeta {
+  uint64_t a, b;
+};
+
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
+__device__ __forceinline__ const uint64_t* meta_row(uint64_t v) {
+  return reinterpret_cast<const uint64_t*>(v & ~(uint64_t)15);
+}
+
+__device__ __forceinline__ void load_row(Aff& p, uint64_t v) {
+  aff_load(p, meta_row(v));
+  if (v & 1) aff_neg(p);
+}
+
+template <bool kFirst, class M>
+__global__ void __launch_bounds__(kAffThreads, 2) k_msm_affine_round(
+    const MsmJobs J, const uint2* pairs, const uint64_t* in_pts, const uint32_t* in_ends,
+    const uint32_t* out_ends, int keys, int k, uint64_t* out_pts, uint64_t* scratch, AffMeta* meta,
+    uint2* out_pairs) {
+  G1F f;
+  __shared__ uint32_t s_wtot[3][kAffWorkerWarps][8];
+  __shared__ uint32_t s_wpre[3][kAffWorkerWarps][8], s_wsuf[3][kAffWorkerWarps][8];
+  __shared__ uint32_t s_inv[3][8];
+  __shared__ uint32_t s_others[3][kAffWorkers][8];  // per worker: the product of its warp's other chains
+  const uint32_t total = out_ends[keys - 1];
+  const int64_t per_batch = (int64_t)kAffWorkers * k;
+  // batches of this block: b, b + G, ... while their first entry is below total (uniform in the block)
+  int64_t nb = 0;
+  if ((int64_t)blockIdx.x * per_batch < (int64_t)total) {
+    nb = ((int64_t)total - (int64_t)blockIdx.x * per_batch + (int64_t)gridDim.x * per_batch - 1) /
+         ((int64_t)gridDim.x * per_batch);
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const bool worker = w < kAffWorkerWarps;
+  const int wi = worker ? (int)threadIdx.x : 0;
+  const int64_t nw_grid = (int64_t)gridDim.x * kAffWorkers;
+  const int64_t gw = (int64_t)blockIdx.x * kAffWorkers + wi;
+  auto first_entry = [&](int64_t batch) { return (batch * gridDim.x + blockIdx.x) * per_batch + (int64_t)wi * k; };
+  auto count_of = [&](int64_t e0) {
+    return e0 < (int64_t)total ? (int)min((int64_t)k, (int64_t)total - e0) : 0;
+  };
+  // the source rows of output entry e (bucket walk from *b)
+  auto resolve = [&](uint32_t e, int* b, AffMeta* m, bool* pair) {
+    while (out_ends[*b] <= e) ++*b;
+    const uint32_t ostart = *b ? out_ends[*b - 1] : 0u;
+    const uint32_t istart = *b ? in_ends[*b - 1] : 0u;
+    const uint32_t in = istart + 2u * (e - ostart);
+    *pair = in + 1u < in_ends[*b];
+    if (kFirst) {
+      const uint2 kv1 = pairs[in];
+      const JobPoints jp = job_points(J, kv1.x);
+      const int64_t i1 = (int64_t)(kv1.y & 0x7fffffffu);
+      m->a = reinterpret_cast<uint64_t>(i1 < jp.n ? jp.points + 8 * i1 : jp.phi + 8 * (i1 - jp.n)) | (kv1.y >> 31);
+      m->b = 0;
+      if (*pair) {
+        const uint2 kv2 = pairs[in + 1u];
+        const int64_t i2 = (int64_t)(kv2.y & 0x7fffffffu);
+        m->b = reinterpret_cast<uint64_t>(i2 < jp.n ? jp.points + 8 * i2 : jp.phi + 8 * (i2 - jp.n)) | (kv2.y >> 31);
+      }
+    } else {
+      m->a = reinterpret_cast<uint64_t>(in_pts + 8 * (int64_t)in);
+      m->b = *pair ? m->a + 64 : 0;
+    }
+  };
+
+  int64_t e0_1 = 0, e0_2 = 0;  // first entries of batches t - 1 and t - 2
+  int cnt_1 = 0, cnt_2 = 0;
+  uint32_t acc[8];
+
+  for (int64_t t = 0; t <= nb + 1; ++t) {
+    const int qf = (int)(t % 3), qb = (int)((t + 1) % 3), qi = (int)((t + 2) % 3);  // batches t, t - 2, t - 1
+    if (worker) {
+      const bool fwd = t < nb, bwd = t >= 2 && cnt_2 > 0;
+      const int64_t e0 = fwd ? first_entry(t) : 0;
+      const int n_f = fwd ? count_of(e0) : 0;
+      const int n_b = bwd ? cnt_2 : 0;
+      uint64_t* fscr = scratch + 4 * (int64_t)qf * k * nw_grid;
+      AffMeta* fmet = meta + (int64_t)qf * k * nw_grid;
+      const uint64_t* bscr = scratch + 4 * (int64_t)qb * k * nw_grid;
+      const AffMeta* bmet = meta + (int64_t)qb * k * nw_grid;
+      fe_one(acc, f);
+      uint32_t inv[8];
+      if (n_b > 0) {
+        M::mul(inv, s_inv[qb], s_wpre[qb][w]);
+        M::mul(inv, inv, s_wsuf[qb][w]);
+        M::mul(inv, inv, s_others[qb][wi]);  // = 1 / (this thread's chain of batch t - 2)
+      }
+      // forward look-ahead: entry 0 resolved and its rows on their way to L2
+      int fb = n_f > 0 ? bucket_of_entry(out_ends, keys, (uint32_t)e0) : 0;
+      AffMeta fm{0, 0};
+      bool fpair = false;
+      if (n_f > 0) {
+        resolve((uint32_t)e0, &fb, &fm, &fpair);
+        prefetch_l2(meta_row(fm.a));
+        if (fpair) prefetch_l2(meta_row(fm.b));
+      }
+      AffMeta bm{0, 0};
+      if (n_b > 0) {
+        bm = bmet[(int64_t)(n_b - 1) * nw_grid + gw];
+        prefetch_l2(meta_row(bm.a));
+        if (bm.b) prefetch_l2(meta_row(bm.b));
+      }
+      const int steps = n_f > n_b ? n_f : n_b;
+      for (int i = 0; i < steps; ++i) {
+        // ---- forward entry i: its x coordinates start loading now ----
+        uint32_t x1[8], x2[8];
+        const AffMeta cur = fm;
+        const bool cur_pair = fpair;
+        const int cur_b = fb;  // entry i's bucket (fb moves on to entry i + 1's below)
+        if (i < n_f) {
+          fe_load(x1, meta_row(cur.a));
+          if (cur_pair) fe_load(x2, meta_row(cur.b));
+          if (i + 1 < n_f) {  // resolve entry i + 1 and prefetch its rows
+            resolve((uint32_t)(e0 + i + 1), &fb, &fm, &fpair);
+            prefetch_l2(meta_row(fm.a));
+            if (fpair) prefetch_l2(meta_row(fm.b));
+          }
+        }
+        // ---- backward entry n_b - 1 - i of batch t - 2 ----
+        if (i < n_b) {
+          const int bi = n_b - 1 - i;
+          const AffMeta m = bm;
+          if (bi > 0) {
+            bm = bmet[(int64_t)(bi - 1) * nw_grid + gw];
+            prefetch_l2(meta_row(bm.a));
+            if (bm.b) prefetch_l2(meta_row(bm.b));
+          }
+          const uint32_t cs = (uint32_t)(m.a >> 1) & 7u;
+          uint64_t* dst = out_pts + 8 * (e0_2 + bi);
+          if (cs == kAffInf) {
+            aff_store_inf(dst);
+          } else if (cs == kAffCopy1 || cs == kAffCopy2) {
+            Aff p;
+            load_row(p, cs == kAffCopy1 ? m.a : m.b);
+            fe_store(dst, p.x);
+            fe_store(dst + 4, p.y);
+          } else {
+            uint32_t inv_i[8];
+            if (bi > 0) {
+              uint32_t prev[8];
+              fe_load(prev, bscr + 4 * ((int64_t)(bi - 1) * nw_grid + gw));
+              M::mul(inv_i, inv, prev);
+            } else {
+              fe_copy(inv_i, inv);
+            }
+            Aff p1, p2;
+            load_row(p1, m.a);
+            uint32_t d[8], lam[8], x3[8], y3[8];
+            if (cs == kAffAdd) {
+              load_row(p2, m.b);
+              fe_sub(d, p2.x, p1.x, f);
+              fe_sub(lam, p2.y, p1.y, f);
+            } else {
+              fe_dbl(d, p1.y, f);
+              M::sqr(lam, p1.x);
+              uint32_t t2[8];
+              fe_dbl(t2, lam, f);
+              fe_add(lam, lam, t2, f);  // 3 x1^2
+              fe_copy(p2.x, p1.x);
+            }
+            if (bi > 0) M::mul(inv, inv, d);  // now 1 / (the chain before entry bi)
+            M::mul(lam, lam, inv_i);
+            M::sqr(x3, lam);
+            fe_sub(x3, x3, p1.x, f);
+            fe_sub(x3, x3, p2.x, f);
+            fe_sub(y3, p1.x, x3, f);
+            M::mul(y3, lam, y3);
+            fe_sub(y3, y3, p1.y, f);
+            fe_store(dst, x3);
+            fe_store(dst + 4, y3);
+          }
+        }
+        // ---- forward entry i: its denominator joins the chain ----
+        if (i < n_f) {
+          uint32_t d[8], cs;
+          if (!cur_pair) {
+            fe_one(d, f);
+            cs = kAffCopy1;
+          } else {
+            const bool i1 = (x1[7] >> 31) != 0, i2 = (x2[7] >> 31) != 0;
+            if (i1 || i2) {
+              fe_one(d, f);
+              cs = i1 && i2 ? kAffInf : (i1 ? kAffCopy2 : kAffCopy1);
+            } else {
+              fe_sub(d, x2, x1, f);
+              cs = kAffAdd;
+              if (fe_is_zero(d)) {
+                Aff q1, q2;
+                load_row(q1, cur.a);
+                load_row(q2, cur.b);
+                if (fe_eq(q1.y, q2.y) && !fe_is_zero(q1.y)) {
+                  fe_dbl(d, q1.y, f);
+                  cs = kAffDbl;
+                } else {
+                  fe_one(d, f);
+                  cs = kAffInf;
+                }
+              }
+            }
+          }
+          if (i == 0) {
+            fe_copy(acc, d);
+          } else {
+            M::mul(acc, acc, d);
+          }
+          fe_store(fscr + 4 * ((int64_t)i * nw_grid + gw), acc);
+          fmet[(int64_t)i * nw_grid + gw] = AffMeta{cur.a | ((uint64_t)cs << 1), cur.b};
+          if (out_pairs) out_pairs[e0 + i] = make_uint2((uint32_t)cur_b, (uint32_t)(e0 + i));
+        }
+      }
+      // the forward chain's place among the block's chains (every worker lane joins)
+      if (fwd) {
+        uint32_t xp[8], xs[8], o[8];
+        warp_exclusive_products<M>(xp, xs, acc, lane);
+        M::mul(o, xp, xs);
+        fe_copy(s_others[qf][wi], o);
+        if (lane == 31) {
+          uint32_t tot[8];
+          M::mul(tot, xp, acc);
+          fe_copy(s_wtot[qf][w], tot);
+        }
+      }
+      e0_2 = e0_1;
+      cnt_2 = cnt_1;
+      e0_1 = e0;
+      cnt_1 = n_f;
+    } else if (t >= 1 && t <= nb) {
+      // ---- warp 7: combine the worker warps of batch t - 1 and invert it ----
+      uint32_t v[8], xp[8], xs[8];
+      if (lane < kAffWorkerWarps) {
+        fe_copy(v, s_wtot[qi][lane]);
+      } else {
+        fe_one(v, f);
+      }
+      warp_exclusive_products<M>(xp, xs, v, lane);
+      if (lane < kAffWorkerWarps) {
+        fe_copy(s_wpre[qi][lane], xp);
+        fe_copy(s_wsuf[qi][lane], xs);
+      }
+      uint32_t tot[8], inv[8];
+      M::mul(tot, xp, v);  // lane 6: the product of all seven warps
+#pragma unroll
+      for (int c = 0; c < 8; ++c) tot[c] = __shfl_sync(0xffffffffu, tot[c], kAffWorkerWarps - 1);
+      fe_inv(inv, tot, f);  // never zero: every factor is nonzero
+      if (lane == 0) fe_copy(s_inv[qi], inv);
+    }
+    __syncthreads();
+  }
 }
 
 // Levels 2+: K2 slots per thread, full XYZZ additions; slots without a key
@@ -771,14 +1122,26 @@ struct MsmPlan {
   int64_t windows = 0;    // bucket sets of the batch: count W, or count with tables
   int64_t keys_used = 0;  // bucket keys of the batch (count * W * 2^(w-1))
   int64_t E = 0;   // sorted pairs
+  int aff_rounds = 0;               // affine rounds before the XYZZ levels ("msm.affine_rounds")
+  int aff_k = 64;                   // output entries per thread of an affine round ("msm.affine_batch")
+  std::vector<int64_t> aff_bound;   // bound on each round's list: aff_bound[0] = E, then per round
+  int64_t E_list = 0;               // entries the XYZZ levels start from (E, or the last round's bound)
   int64_t T1 = 0;  // level-1 threads
   std::vector<int64_t> slot_levels;  // thread count of each merge level
   size_t cub_bytes = 0;
   // workspace offsets
   size_t off_keys0, off_keys1, off_vals0, off_vals1, off_cub, off_phi, off_buckets,
       off_slot_keys_a, off_slot_pts_a, off_slot_keys_b, off_slot_pts_b, off_red_s0, off_red_u0,
-      off_red_s1, off_red_u1, off_wsum, off_counts, off_offsets, total;
+      off_red_s1, off_red_u1, off_wsum, off_counts, off_offsets, off_aff_ends0, off_aff_ends1,
+      off_aff_half, off_aff_pts0, off_aff_pts1, off_aff_scratch, off_aff_meta, total;
 };
+
+// Blocks of an affine round over a list of `entries`: persistent, at most two per
+// SM (their register budget), and no more than the batches of 224 k entries.
+static int64_t aff_blocks(int64_t entries, int k) {
+  const int64_t per = (int64_t)kAffWorkers * k;
+  return std::max<int64_t>(1, std::min<int64_t>((entries + per - 1) / per, 2 * 148));
+}
 
 // Plan for a batch of jobs with point counts sizes[0..count) at window w.
 static int make_plan(const int64_t* sizes, int count, int w, MsmPlan& p, int table = 0, int k1 = 0,
@@ -801,6 +1164,25 @@ static int make_plan(const int64_t* sizes, int count, int w, MsmPlan& p, int tab
   p.keys_used = keys_used;
   p.counting_sort = table ? 1 : tune_get("msm.sort");
   p.E = 2 * (int64_t)p.W * n;  // both GLV halves
+  // Affine rounds (counting sort only: they start from its bucket ends). By
+  // default a round runs while its list still fills every SM with two blocks of
+  // full batches; "msm.affine_rounds" > 0 forces that many at any size, 0 turns
+  // them off. A round's list has at most sum ceil(n_b / 2) <= B / 2 + keys / 2
+  // entries.
+  p.aff_k = tune_get("msm.affine_batch");
+  const int forced = tune_get("msm.affine_rounds");
+  p.aff_bound.assign(1, p.E);
+  if (p.counting_sort && forced != 0) {
+    const int64_t min_out = (int64_t)2 * 148 * kAffWorkers * p.aff_k;
+    for (int r = 0; r < 8; ++r) {
+      const int64_t b = p.aff_bound.back();
+      const int64_t nb = std::min(b, (b + 1) / 2 + (keys_used + 1) / 2);
+      if (forced > 0 ? r >= forced : nb < min_out) break;
+      p.aff_bound.push_back(nb);
+    }
+  }
+  p.aff_rounds = (int)p.aff_bound.size() - 1;
+  p.E_list = p.aff_bound.back();
   // pairs per level-1 thread: the knob, else by size. A thread adds its pairs one
   // after another, so small MSMs want short chains and many threads; each thread
   // may leave two partial sums for the merge levels, so large ones want long
@@ -812,12 +1194,12 @@ static int make_plan(const int64_t* sizes, int count, int w, MsmPlan& p, int tab
   p.k1 = k1 > 0 ? k1 : tune_get("msm.pairs_per_thread");
   if (p.k1 < 8) {
     p.k1 = 8;
-    while (p.k1 < 64 && ((int64_t)p.k1 << 20) <= p.E) p.k1 <<= 1;
+    while (p.k1 < 64 && ((int64_t)p.k1 << 20) <= p.E_list) p.k1 <<= 1;
   }
   p.k2 = tune_get("msm.slots_per_thread");
   p.log_l = log_l > 0 ? log_l : tune_get("msm.reduce_log_segment");
   p.call_products = tune_get("msm.call_products");
-  p.T1 = (p.E + p.k1 - 1) / p.k1;
+  p.T1 = (p.E_list + p.k1 - 1) / p.k1;
   p.slot_levels.clear();
   int64_t M = 2 * p.T1;
   int64_t T = p.T1;
@@ -837,6 +1219,13 @@ static int make_plan(const int64_t* sizes, int count, int w, MsmPlan& p, int tab
                                       (int)(keys_used + 1), (cudaStream_t)0);
   if (err != cudaSuccess) return check_cuda(err, "CUB scan size query");
   p.cub_bytes = cub_bytes > scan_bytes ? cub_bytes : scan_bytes;
+  if (p.aff_rounds > 0) {
+    size_t incl_bytes = 0;
+    err = cub::DeviceScan::InclusiveSum(nullptr, incl_bytes, (const uint32_t*)nullptr, (uint32_t*)nullptr,
+                                        (int)keys_used, (cudaStream_t)0);
+    if (err != cudaSuccess) return check_cuda(err, "CUB scan size query");
+    p.cub_bytes = std::max(p.cub_bytes, incl_bytes);
+  }
 
   size_t off = 0;
   auto take = [&](size_t bytes) {
@@ -866,6 +1255,20 @@ static int make_plan(const int64_t* sizes, int count, int w, MsmPlan& p, int tab
   // counting sort: per-key counts, then offsets / cursors (one more entry: the total)
   p.off_counts = take((size_t)(keys_used + 1) * 4);
   p.off_offsets = take((size_t)(keys_used + 1) * 4);
+  // affine rounds: two bucket-end arrays and the halved counts, two point lists
+  // (rounds alternate), and the per-entry chain prefixes and cases of the
+  // largest round (round 0)
+  const bool aff = p.aff_rounds > 0;
+  p.off_aff_ends0 = take(aff ? (size_t)keys_used * 4 : 0);
+  p.off_aff_ends1 = take(aff ? (size_t)keys_used * 4 : 0);
+  p.off_aff_half = take(aff ? (size_t)keys_used * 4 : 0);
+  p.off_aff_pts0 = take(aff ? (size_t)p.aff_bound[1] * 64 : 0);
+  p.off_aff_pts1 = take(p.aff_rounds >= 2 ? (size_t)p.aff_bound[2] * 64 : 0);
+  // three batches in flight per worker thread (one being chained, one being
+  // inverted, one being walked back): 3 k chain prefixes and source records each
+  const int64_t aff_entries = aff ? 3 * aff_blocks(p.aff_bound[1], p.aff_k) * kAffWorkers * p.aff_k : 0;
+  p.off_aff_scratch = take((size_t)aff_entries * 32);
+  p.off_aff_meta = take((size_t)aff_entries * 16);
   p.total = off;
   return ZKB_OK;
 }
@@ -902,6 +1305,7 @@ static int run_msm(const MsmJobs& J, const MsmPlan& p, char* ws, cudaStream_t s)
   const uint32_t* svals = vals1;
   int st = 1;
   const uint32_t* e_dev = nullptr;  // pairs written by the counting sort (device)
+  const uint64_t* list_pts = nullptr;  // after affine rounds: the points the final list indexes
   if (p.counting_sort) {
     uint32_t* counts = reinterpret_cast<uint32_t*>(ws + p.off_counts);
     uint32_t* offsets = reinterpret_cast<uint32_t*>(ws + p.off_offsets);
@@ -931,6 +1335,49 @@ static int run_msm(const MsmJobs& J, const MsmPlan& p, char* ws, cudaStream_t s)
     skeys = keys0;
     svals = keys0 + 1;
     st = 2;
+    if (p.aff_rounds > 0) {
+      // after the scatter, offsets[b] is the end of bucket b's pairs
+      ProfSpan aspan("msm_affine_rounds", s);
+      const int keys = (int)p.keys_used;
+      const uint32_t* in_ends = offsets;
+      const uint64_t* in_pts = nullptr;
+      uint32_t* ends[2] = {reinterpret_cast<uint32_t*>(ws + p.off_aff_ends0),
+                           reinterpret_cast<uint32_t*>(ws + p.off_aff_ends1)};
+      uint64_t* pts[2] = {reinterpret_cast<uint64_t*>(ws + p.off_aff_pts0),
+                          reinterpret_cast<uint64_t*>(ws + p.off_aff_pts1)};
+      uint32_t* half = reinterpret_cast<uint32_t*>(ws + p.off_aff_half);
+      uint64_t* scratch = reinterpret_cast<uint64_t*>(ws + p.off_aff_scratch);
+      AffMeta* meta = reinterpret_cast<AffMeta*>(ws + p.off_aff_meta);
+      // the final list's (bucket, entry) pairs take the space of the unused value arrays
+      uint2* final_pairs = reinterpret_cast<uint2*>(ws + p.off_vals0);
+      for (int r = 0; r < p.aff_rounds; ++r) {
+        uint32_t* out_ends = ends[r & 1];
+        k_msm_half_counts<<<grid_for(keys, 256), 256, 0, s>>>(in_ends, keys, half);
+        ZKB_TRY(check_launch("msm affine round counts"));
+        size_t scan_bytes2 = p.cub_bytes;
+        ZKB_TRY(check_cuda(cub::DeviceScan::InclusiveSum(ws + p.off_cub, scan_bytes2, half, out_ends, keys, s),
+                           "msm affine round layout"));
+        const int64_t blocks = aff_blocks(p.aff_bound[r + 1], p.aff_k);
+        uint2* op = r + 1 == p.aff_rounds ? final_pairs : nullptr;
+        if (r == 0) {
+          auto kern = p.call_products ? k_msm_affine_round<true, CallMul> : k_msm_affine_round<true, InlineMul>;
+          kern<<<(unsigned)blocks, kAffThreads, 0, s>>>(J, pairs, in_pts, in_ends, out_ends, keys, p.aff_k, pts[0],
+                                                         scratch, meta, op);
+        } else {
+          auto kern = p.call_products ? k_msm_affine_round<false, CallMul> : k_msm_affine_round<false, InlineMul>;
+          kern<<<(unsigned)blocks, kAffThreads, 0, s>>>(J, nullptr, in_pts, in_ends, out_ends, keys, p.aff_k,
+                                                         pts[r & 1], scratch, meta, op);
+        }
+        ZKB_TRY(check_launch("msm affine round"));
+        in_ends = out_ends;
+        in_pts = pts[r & 1];
+      }
+      // the XYZZ levels take the last round's points as one point array
+      list_pts = in_pts;
+      skeys = reinterpret_cast<const uint32_t*>(final_pairs);
+      svals = skeys + 1;
+      e_dev = in_ends + keys - 1;
+    }
   } else {
     {
       ProfSpan span("msm_digits", s);
@@ -960,7 +1407,17 @@ static int run_msm(const MsmJobs& J, const MsmPlan& p, char* ws, cudaStream_t s)
   {
     ProfSpan span("msm_acc_points", s);
     const unsigned grid = (unsigned)((p.T1 + 127) / 128);
-    if (p.count > 1) {
+    if (list_pts) {
+      // one point array for every job: the one-job kernel over a job table whose
+      // only entry is that array
+      MsmJobs L = J;
+      L.count = 1;
+      L.points[0] = list_pts;
+      L.phi[0] = nullptr;
+      L.pts_n[0] = INT64_MAX;
+      auto kern = p.call_products ? k_msm_acc_points<CallMul> : k_msm_acc_points<InlineMul>;
+      kern<<<grid, 128, 0, s>>>(L, skeys, svals, st, p.E_list, e_dev, p.k1, p.none, buckets, sk[0], sp[0]);
+    } else if (p.count > 1) {
       auto kern = p.call_products ? k_msm_acc_points_batch<CallMul> : k_msm_acc_points_batch<InlineMul>;
       kern<<<grid, 128, 0, s>>>(J, skeys, svals, st, p.E, e_dev, p.k1, p.none, buckets, sk[0], sp[0]);
     } else {

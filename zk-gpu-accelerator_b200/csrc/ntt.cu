@@ -539,10 +539,12 @@ __global__ void __launch_bounds__(kNttThreads, 1) k_ntt_pass(F f, NttPass a) {
 // The pass kernel fed by TMA (the default for transforms of two or more passes)
 // ---------------------------------------------------------------------------
 //
-// Persistent: each CTA takes tiles blockIdx.x, blockIdx.x + gridDim.x, ...
-// One thread issues the tile's tensor loads (cp.async.bulk.tensor) into a
-// shared-memory buffer and the copies complete on that buffer's mbarrier; with
-// two buffers the loads of the CTA's next tile run while this tile computes.
+// Each CTA takes tiles blockIdx.x, blockIdx.x + gridDim.x, ...: by default one
+// tile per CTA (a grid of all tiles), or one persistent wave ("ntt.tma_grid" =
+// 0). One thread issues the tile's tensor loads (cp.async.bulk.tensor) into a
+// shared-memory buffer and the copies complete on that buffer's mbarrier; in
+// the persistent form two buffers let the loads of the CTA's next tile run
+// while this tile computes.
 // A tile is C columns of R rows in natural order, split into two planes of
 // 16-byte half-elements (the low and the high 16 bytes of each 32-byte row),
 // so that consecutive rows read by consecutive lanes fall into distinct banks.
@@ -585,9 +587,9 @@ __device__ __forceinline__ void plane_store(uint4* lo, uint4* hi, int i, const u
   hi[i] = make_uint4(x[4], x[5], x[6], x[7]);
 }
 
-template <class F>
-__global__ void __launch_bounds__(kNttThreads) k_ntt_pass_tma(F f, const NttPass a, const TmaPass tp,
-                                                             const __grid_constant__ CUtensorMap tmap) {
+template <class F, int kThreads = kNttThreads, int kMinBlocks = 1>
+__global__ void __launch_bounds__(kThreads, kMinBlocks) k_ntt_pass_tma(F f, const NttPass a, const TmaPass tp,
+                                                                      const __grid_constant__ CUtensorMap tmap) {
   extern __shared__ __align__(1024) unsigned char smem_raw_tma[];
   // the buffers start on a 1 KiB boundary (the launch asks for 1 KiB more)
   unsigned char* smem_tma = smem_raw_tma + ((1024u - (smem_u32(smem_raw_tma) & 1023u)) & 1023u);
@@ -1298,18 +1300,25 @@ static int launch_pass_tma(const F& f, const PassLaunch& L, int64_t n, int P, in
     ZKB_TRY(encode_tensor_map_u64(&map, a.in, 3, dims, strides, box));
     tp.four_d = 0;
   }
+  // One tile per block ("ntt.tma_grid" = 1, the default) lets the block scheduler
+  // refill each SM as its blocks finish; measured on B200 against one persistent
+  // wave of double-buffered blocks: 2^24 rows 4.97 against 5.29 ms (and against
+  // 5.27 ms for the per-thread gather form), 2^22 1.19 against 1.25 ms.
+  const bool per_tile = tune_get("ntt.tma_grid") != 0;
   const size_t plane = (size_t)T * 16;
   const size_t rest = ((size_t)R >> 1) * 32 + 2 * 8 + 1024;  // stage table, barriers, alignment slack
-  tp.nbuf = 4 * plane + rest <= (110u << 10) ? 2 : 1;
+  tp.nbuf = !per_tile && 4 * plane + rest <= (110u << 10) ? 2 : 1;
   const size_t smem = (size_t)tp.nbuf * 2 * plane + rest;
-  auto kern = k_ntt_pass_tma<F>;
+  // 128-thread blocks may take a register cap for 5 or 6 blocks per SM ("ntt.tma_blocks_per_sm")
+  const int cap = L.threads == 128 ? tune_get("ntt.tma_blocks_per_sm") : 0;
+  auto kern = cap == 6 ? k_ntt_pass_tma<F, 128, 6> : cap == 5 ? k_ntt_pass_tma<F, 128, 5> : k_ntt_pass_tma<F>;
   ZKB_TRY(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                      "NTT pass shared memory attribute"));
   int per_sm = 0;
   ZKB_TRY(check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, L.threads, smem),
                      "NTT pass occupancy"));
   if (per_sm < 1) return fail(ZKB_ECUDA, "NTT pass of %d threads and %zu bytes does not fit an SM", L.threads, smem);
-  const int64_t grid = std::min<int64_t>(tp.ntiles, (int64_t)sms * per_sm);
+  const int64_t grid = per_tile ? tp.ntiles : std::min<int64_t>(tp.ntiles, (int64_t)sms * per_sm);
   ProfSpan span(a.last ? "ntt_last_pass" : "ntt_column_pass", s);
   (void)q;
   kern<<<(unsigned)grid, L.threads, smem, s>>>(f, a, tp, map);

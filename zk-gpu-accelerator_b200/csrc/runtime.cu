@@ -27,6 +27,8 @@ static Knob g_knobs[] = {
     {"msm.reduce_log_segment", 1, 1, 8},     // log2 of the running-sum segment length
     {"msm.call_products", 1, 0, 1},          // bucket kernels call one shared product (1) or inline all (0)
     {"msm.sort", 1, 0, 1},                   // pairs grouped by a counting sort (1) or a radix sort (0)
+    {"msm.affine_rounds", 0, -1, 8},         // affine rounds before the XYZZ levels (0 = none, -1 = by size)
+    {"msm.affine_batch", 64, 8, 512},        // output entries per thread of an affine round
     {"ntt.max_log_radix", 0, 0, 12},         // largest sub-transform per pass (log2, 8..12; 0 = by size)
     {"ntt.cta_log_elems", 0, 0, 12},         // elements staged per CTA (log2, 9..12; 0 = by size)
     {"ntt.threads", 0, 0, 512},              // threads per NTT CTA (64..512; 0 = by tile)
@@ -34,6 +36,8 @@ static Knob g_knobs[] = {
     {"ntt.full_table_mb", 4096, 0, 65536},   // budget of expanded NTT tables (MiB; 0 = two-level only)
     {"ntt.batch_spin_limit", 0, 0, 1 << 30},  // polls before a batch tile's dependency wait gives up (0 = 2^22)
     {"ntt.tma", 1, 0, 1},                    // multi-pass transforms: TMA-fed persistent passes (1) or per-thread gathers (0)
+    {"ntt.tma_grid", 1, 0, 1},               // TMA passes: one persistent wave (0) or one tile per block (1)
+    {"ntt.tma_blocks_per_sm", 0, 0, 6},      // TMA passes of 128-thread blocks: registers capped for 5 or 6 blocks (0 = no cap)
     {"ntt64.first_col_log", -1, -1, 6},      // int64 NTT first pass: log2 of input words per row (-1 = by size)
     {"ntt64.first_max_k", 0, 0, 10},         // int64 NTT first pass: stages (4..10; 0 = by size)
     {"ntt64.col_log", 0, 0, 6},              // int64 NTT later passes: log2 of words per row (1..6; 0 = by size)
