@@ -661,9 +661,9 @@ def _profile_traffic(kernel: str, n: int) -> float | None:
 def _run_e2e(args, step: Step, dist, device, log_msm: int, log_ntt: int) -> dict:
     """The same step through the public API with pinned host inputs and host results.
 
-    The timed form stages the step's inputs over PCIe on one copy stream, longest
-    work first: the uniform scalars with the base set (copied once, shared by both
-    MSMs), the skewed scalars, then the two NTT inputs. The four public-API calls
+    The timed form stages the step's inputs over PCIe on one copy stream: the
+    uniform scalars with the base set (copied once, shared by both MSMs), the two
+    NTT inputs, then the skewed scalars. The four public-API calls
     (msm_pippenger_affine x2, to_montgomery / ntt / from_montgomery x2) are issued
     from four host threads, each on its own stream waiting for its own inputs; the
     NTT streams have the higher priority, so each transform finishes soon after
@@ -713,17 +713,20 @@ def _run_e2e(args, step: Step, dist, device, log_msm: int, log_ntt: int) -> dict
     start = torch.cuda.Event(enable_timing=True)
 
     def stage_inputs() -> None:
+        # the longest MSM's inputs first, then both NTT inputs, the skewed scalars last:
+        # each transform's 512 MB result then crosses PCIe back while the MSMs still
+        # compute (measured on B200: 46.8 against 49.2 ms with the skewed scalars second)
         copy.wait_event(start)
         with torch.cuda.stream(copy):
             su_dev.copy_(su, non_blocking=True)
             b_dev.copy_(plain, non_blocking=True)
             ready[0].record(copy)
-            ss_dev.copy_(ss, non_blocking=True)
-            ready[1].record(copy)
             x_dev[0].copy_(xin, non_blocking=True)
             ready[2].record(copy)
             x_dev[1].copy_(xin, non_blocking=True)
             ready[3].record(copy)
+            ss_dev.copy_(ss, non_blocking=True)
+            ready[1].record(copy)
 
     def on_stream(i: int, staged: bool) -> None:
         torch.cuda.set_device(device)
@@ -777,8 +780,9 @@ def _run_e2e(args, step: Step, dist, device, log_msm: int, log_ntt: int) -> dict
             "api_copies_ms": round(api_ms, 3), "api_copies_h2d_bytes_per_step": int(h2d_api),
             "sequential_ms": round(seq, 3), "same_results": same,
             "api": "zkgpu.msm_gpu.msm_pippenger_affine x2, Field256.to_montgomery/ntt/from_montgomery x2 from four "
-                   "host threads on four streams, inputs staged on one copy stream, MSM inputs first (the "
-                   "base set copied once), then the NTT inputs; NTTs on high-priority streams; api_copies_ms: the same calls "
+                   "host threads on four streams, inputs staged on one copy stream: the uniform MSM's inputs (the "
+                   "base set copied once), the NTT inputs, the skewed scalars; NTTs on high-priority streams; "
+                   "api_copies_ms: the same calls "
                    "given the host tensors (each copies its own inputs); sequential_ms: one after another"}
 
 
@@ -874,10 +878,17 @@ def _event_ms(fn, reps: int) -> float:
     return a.elapsed_time(b) / reps
 
 
-def run_batched(seed: int = 6, log_base: int = 20) -> dict:
+def run_batched(seed: int = 6, log_base: int = 20, table_windows: tuple[int, ...] = (15, 16, 17)) -> dict:
     """64 Fr NTTs (sizes 2^U{10..20}, uniform inputs) + 32 G1 MSMs (sizes 2^U(12, 20) over
-    prefixes of one resident 2^20 base set, uniform scalars): one-at-a-time calls against one
-    BatchPlan run (one persistent NTT launch + one MSM batch) and its CUDA-graph replay."""
+    prefixes of one resident 2^20 base set, uniform scalars): one-at-a-time calls (zkb_ntt and
+    zkb_msm per job, the drop-in path) against one BatchPlan run (one persistent NTT launch + one
+    MSM batch) and its CUDA-graph replay.
+
+    The batch is tuned for its shape: the MSM jobs share the resident base set, so the batch
+    runs them over a fixed-base table of it, and the table's window is chosen by timing the
+    whole batch at each candidate window (`autotune`); the variable-base batch, with the
+    library's per-size windows, is timed beside it, and so is one call per job over the chosen
+    table, so the ratio of every form is on the line."""
     import ctypes
 
     import numpy as np
@@ -885,6 +896,7 @@ def run_batched(seed: int = 6, log_base: int = 20) -> dict:
 
     from zkgpu import _native, batch, curve_gpu, workloads as wl
     from zkgpu.field256_gpu import BN254_FR
+    from zkgpu.msm_gpu import FixedBaseTable
 
     rng = np.random.default_rng(seed)
     ntt_sizes = [1 << int(v) for v in rng.integers(10, log_base + 1, size=64)]
@@ -908,24 +920,75 @@ def run_batched(seed: int = 6, log_base: int = 20) -> dict:
             _native.check(lib.zkb_msm(bases.data_ptr(), scs[k].data_ptr(), n, 0, res[k].data_ptr(),
                                       msm_ws[k].data_ptr(), msm_ws[k].numel(), s))
 
-    plan = batch.BatchPlan(ntt_jobs=[(x, False, None) for x in xs],
-                           msm_jobs=[(bases[:n], scs[k], None) for k, n in enumerate(msm_sizes)])
     t_plain = _event_ms(plain, 3)
-    t_batch = _event_ms(plan.run, 3)
-    same = all(bool((o == y).all()) for o, y in zip(outs, plan.ntt_outputs)) and \
-        bool((res[:, :9] == plan.msm_results[:32, :9]).all())
+    ntt_jobs = [(x, False, None) for x in xs]
+    msm_jobs = [(bases[:n], scs[k], None) for k, n in enumerate(msm_sizes)]
+
+    def check(plan) -> bool:
+        return all(bool((o == y).all()) for o, y in zip(outs, plan.ntt_outputs)) and \
+            bool((res[:, :9] == plan.msm_results[:32, :9]).all())
+
+    # the variable-base batch (per-size windows, one pipeline per window group)
+    vplan = batch.BatchPlan(ntt_jobs=ntt_jobs, msm_jobs=msm_jobs)
+    t_var = _event_ms(vplan.run, 3)
+    same = check(vplan)
+    del vplan
+    # the table window, tuned for this batch by timing it
+    tuned: dict[int, float] = {}
+    build_ms: dict[int, float] = {}
+    best = None
+    for w in table_windows:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        table = FixedBaseTable(bases, w)
+        torch.cuda.synchronize()
+        build_ms[w] = (time.perf_counter() - t0) * 1e3
+        plan = batch.BatchPlan(ntt_jobs=ntt_jobs, msm_jobs=msm_jobs, table=table)
+        tuned[w] = _event_ms(plan.run, 3)
+        same = same and check(plan)
+        if best is None or tuned[w] < tuned[best[0]]:
+            best = (w, table, plan)
+        else:
+            del plan, table
+    w_best, table, plan = best
+    t_batch = tuned[w_best]
     plan.capture()
     t_graph = _event_ms(plan.replay, 3)
     plan.check_status()
-    same = same and all(bool((o == y).all()) for o, y in zip(outs, plan.ntt_outputs)) and \
-        bool((res[:, :9] == plan.msm_results[:32, :9]).all())
+    same = same and check(plan)
+    # one call per job over the same table (the batch's MSM algorithm without the batching)
+    single = []
+    for k, n in enumerate(msm_sizes):
+        j = (_native.ZkbMsmJob * 1)()
+        j[0].points, j[0].scalars, j[0].n = _native.ptr(table.table), scs[k].data_ptr(), n
+        j[0].result, j[0].window_size = res[k].data_ptr(), w_best
+        single.append((j, _native.workspace(lib.zkb_msm_fixed_batch_workspace_bytes(j, 1))))
+
+    def plain_table() -> None:
+        s = _native.stream_ptr()
+        for k, n in enumerate(ntt_sizes):
+            _native.check(lib.zkb_ntt(ctypes.byref(f), xs[k].data_ptr(), outs[k].data_ptr(), n, 0, None, None,
+                                      ntt_ws[k].data_ptr(), ntt_ws[k].numel(), s))
+        for j, ws in single:
+            _native.check(lib.zkb_msm_fixed_batch(j, 1, ws.data_ptr(), ws.numel(), s))
+
+    t_plain_table = _event_ms(plain_table, 3)
     jobs = len(ntt_sizes) + len(msm_sizes)
+    best_ms = min(t_batch, t_graph)
     return {
         "workload": f"64 Fr NTTs 2^U{{10..{log_base}}} + 32 G1 MSMs 2^U(12,{log_base}) over one resident "
                     f"2^{log_base} base set (seed {seed})",
         "jobs": jobs, "plain_ms": round(t_plain, 3), "batched_ms": round(t_batch, 3), "graph_ms": round(t_graph, 3),
         "plain_jobs_per_s": round(jobs / t_plain * 1e3, 1), "batched_jobs_per_s": round(jobs / t_batch * 1e3, 1),
-        "graph_jobs_per_s": round(jobs / t_graph * 1e3, 1), "speedup": round(t_plain / min(t_batch, t_graph), 3),
+        "graph_jobs_per_s": round(jobs / t_graph * 1e3, 1), "speedup": round(t_plain / best_ms, 3),
+        "plain": "one zkb_ntt / zkb_msm call per job (the drop-in path, variable-base MSMs)",
+        "batched": f"one NTT batch launch + one MSM batch over a fixed-base table of the resident base set "
+                   f"(w = {w_best}, {table.nbytes >> 20} MiB, built once in {build_ms[w_best]:.0f} ms)",
+        "variable_base_batched_ms": round(t_var, 3), "variable_base_speedup": round(t_plain / t_var, 3),
+        "plain_over_table_ms": round(t_plain_table, 3),
+        "speedup_same_msm_algorithm": round(t_plain_table / best_ms, 3),
+        "autotune": {"table_window_ms": {str(k): round(v, 3) for k, v in tuned.items()}, "chosen": w_best,
+                     "how": "the whole batch timed at each candidate table window (CUDA events, mean of 3)"},
         "launches_per_batch": plan.launches_per_run, "same_results": same,
         "timing": "CUDA events, mean of 3 after 2 warm-up",
     }

@@ -218,3 +218,33 @@ def test_ntt_batch_wait_that_runs_out_reports_timeout_then_next_batch_is_exact()
     assert bool((plan.ntt_outputs[0] == want).all())
     fresh = batch.ntt_batch([x])  # the functional form checks the status itself
     assert bool((fresh[0] == want).all())
+
+
+def test_batch_plan_over_a_fixed_base_table_matches_the_plain_batch():
+    """BatchPlan(table=...) runs the MSM jobs over a fixed-base table of the resident base set
+    they are prefixes of; points and rows equal the plain batch's, eager and replayed."""
+    from zkgpu.msm_gpu import FixedBaseTable
+
+    n = 1 << 14
+    bases = curve_gpu.mul_generator(wl.base_scalars(91, n))
+    sizes = [n, 3000, 777, 1 << 12]
+    scs = [wl.uniform_fr(92 + k, m) for k, m in enumerate(sizes)]
+    import torch
+
+    scs = [torch.from_numpy(s).cuda() for s in scs]
+    xs = [_rows_fr(95, 1 << 12), _rows_fr(96, 1 << 9)]
+    ref = batch.BatchPlan(ntt_jobs=[(x, False, None) for x in xs], msm_jobs=[(bases[:m], s, None) for m, s in zip(sizes, scs)])
+    ref.run()
+    for w in (12, 16):
+        table = FixedBaseTable(bases, w)
+        plan = batch.BatchPlan(ntt_jobs=[(x, False, None) for x in xs],
+                               msm_jobs=[(bases[:m], s, None) for m, s in zip(sizes, scs)], table=table)
+        plan.run()
+        assert bool((plan.msm_results[:4, :9] == ref.msm_results[:4, :9]).all()), w
+        assert all(bool((a == b).all()) for a, b in zip(plan.ntt_outputs, ref.ntt_outputs))
+        plan.capture()
+        plan.replay()
+        plan.check_status()
+        assert bool((plan.msm_results[:4, :9] == ref.msm_results[:4, :9]).all()), w
+    with pytest.raises(ValueError, match="table of"):
+        batch.BatchPlan(msm_jobs=[(bases, scs[0], None)], table=FixedBaseTable(bases[:100], 12))

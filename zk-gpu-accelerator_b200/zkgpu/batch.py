@@ -55,12 +55,12 @@ def _ntt_jobs(inputs: Sequence[Any], outputs: Sequence[Any], invert: Sequence[bo
 
 
 def _msm_jobs(points: Sequence[Any], scalars: Sequence[Any], results: Any,
-              window_sizes: Sequence[int | None]) -> Any:
+              window_sizes: Sequence[int | None], counts: Sequence[int] | None = None) -> Any:
     arr = (_native.ZkbMsmJob * max(len(points), 1))()
     for j, (p, s, w) in enumerate(zip(points, scalars, window_sizes, strict=True)):
         arr[j].points = _native.ptr(p)
         arr[j].scalars = _native.ptr(s)
-        arr[j].n = int(p.shape[0])
+        arr[j].n = int(p.shape[0]) if counts is None else int(counts[j])
         arr[j].result = _native.ptr(results) + 8 * _RESULT_WORDS * j
         arr[j].window_size = 0 if w is None else int(w)
     return arr
@@ -204,6 +204,10 @@ class BatchPlan:
 
     ntt_jobs : [(rows, invert, coset)] with rows (n, 4) Montgomery, device
     msm_jobs : [(points, scalars, window_size)] device tensors
+    table    : optional FixedBaseTable of a resident base set whose prefixes every
+               MSM job's points are: the MSMs then run over the table
+               (zkb_msm_fixed_batch, one bucket set per job, no final doublings;
+               the table's window replaces the jobs'), with the same results
     concurrent : run the MSM batch on a high-priority stream and the transforms,
                  one pass launch at a time (zkb_ntt per job), on a low-priority
                  stream beside it. The block scheduler then hands SMs to NTT
@@ -215,7 +219,8 @@ class BatchPlan:
     """
 
     def __init__(self, ntt_jobs: Sequence[tuple[Any, bool, int | None]] = (),
-                 msm_jobs: Sequence[tuple[Any, Any, int | None]] = (), concurrent: bool = False) -> None:
+                 msm_jobs: Sequence[tuple[Any, Any, int | None]] = (), concurrent: bool = False,
+                 table: Any = None) -> None:
         torch = _native.require_cuda()
         self._torch = torch
         self._concurrent = concurrent
@@ -242,9 +247,19 @@ class BatchPlan:
         self.msm_results = torch.zeros((max(len(msm_jobs), 1), _RESULT_WORDS), dtype=torch.int64,
                                        device="cuda")
         self._msm_count = len(msm_jobs)
-        self._msm = (_msm_jobs(self.msm_points, self.msm_scalars, self.msm_results,
-                               [j[2] for j in msm_jobs]) if msm_jobs else None)
-        self._msm_ws_bytes = lib.zkb_msm_batch_workspace_bytes(self._msm, len(msm_jobs)) if msm_jobs else 0
+        self._table = table
+        if table is not None:
+            for p in self.msm_points:
+                if int(p.shape[0]) > table.n:
+                    raise ValueError(f"an MSM of {int(p.shape[0])} points over a table of {table.n}")
+            self._msm = (_msm_jobs([table.table] * len(msm_jobs), self.msm_scalars, self.msm_results,
+                                   [table.window_size] * len(msm_jobs), [int(p.shape[0]) for p in self.msm_points])
+                         if msm_jobs else None)
+            self._msm_ws_bytes = lib.zkb_msm_fixed_batch_workspace_bytes(self._msm, len(msm_jobs)) if msm_jobs else 0
+        else:
+            self._msm = (_msm_jobs(self.msm_points, self.msm_scalars, self.msm_results,
+                                   [j[2] for j in msm_jobs]) if msm_jobs else None)
+            self._msm_ws_bytes = lib.zkb_msm_batch_workspace_bytes(self._msm, len(msm_jobs)) if msm_jobs else 0
         if msm_jobs and _native.last_error():
             raise ValueError(_native.last_error())
         self._msm_ws = _native.workspace(self._msm_ws_bytes)
@@ -275,8 +290,9 @@ class BatchPlan:
                                             _native.ptr(self.status), int(ntt_stream.cuda_stream)),
                           "zkb_ntt_batch")
         if self._msm_count:
-            _native.check(lib.zkb_msm_batch(self._msm, self._msm_count, _native.ptr(self._msm_ws),
-                                            self._msm_ws_bytes, int(msm_stream.cuda_stream)), "zkb_msm_batch")
+            run_fn = lib.zkb_msm_fixed_batch if self._table is not None else lib.zkb_msm_batch
+            _native.check(run_fn(self._msm, self._msm_count, _native.ptr(self._msm_ws), self._msm_ws_bytes,
+                                 int(msm_stream.cuda_stream)), "zkb_msm_batch")
         if split:
             main.wait_stream(self._lo)
             main.wait_stream(self._hi)
