@@ -217,7 +217,13 @@ class Server:
     # ---- footprint ----------------------------------------------------------
 
     def footprint(self, m: int) -> int:
-        """Device bytes one job of size m holds while in flight."""
+        """Device bytes one job of size m holds while in flight (computed once per size)."""
+        cache = self.__dict__.setdefault("_footprints", {})
+        if m not in cache:
+            cache[m] = self._footprint(m)
+        return cache[m]
+
+    def _footprint(self, m: int) -> int:
         lib = _native.lib()
         buffers = (4 + 3 + 3 + 3 + 1 + 1) * m * 32 + 32 * 5
         ntt_ws = 3 * int(lib.zkb_ntt_workspace_bytes(m))
