@@ -67,6 +67,7 @@ WORKLOADS = {
     # name: (log2 MSM points, log2 NTT size)
     "large": (22, 24),
     "small": (20, 22),  # for profiler captures: inputs above the L2 size, ~2 GB on the device
+    "medium": (21, 23),  # for profiler captures whose point set (bases + phi images, 256 MB) exceeds L2
     "tiny": (10, 10),   # for the CPU tests of the reference arm
 }
 
