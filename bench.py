@@ -325,7 +325,7 @@ def init_dist(world: int, backend: str):
     import torch.distributed as dist
 
     os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-    dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=300))
+    dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=180))
     return dist
 
 
