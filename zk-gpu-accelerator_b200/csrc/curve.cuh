@@ -249,6 +249,11 @@ struct InlineMul {
     fe_mul(r, a, b, G1F{});
   }
   __device__ __forceinline__ static void sqr(uint32_t r[8], const uint32_t a[8]) { fe_sqr(r, a, G1F{}); }
+  // r = a b + c d (one Montgomery reduction, fe_mul2)
+  __device__ __forceinline__ static void mul2(uint32_t r[8], const uint32_t a[8], const uint32_t b[8],
+                                              const uint32_t c[8], const uint32_t d[8]) {
+    fe_mul2(r, a, b, c, d, G1F{});
+  }
 };
 
 struct CallMul {
@@ -257,6 +262,10 @@ struct CallMul {
   }
   __device__ __forceinline__ static void sqr(uint32_t r[8], const uint32_t a[8]) {
     fe_sqr_shared(r, a, G1F{});
+  }
+  __device__ __forceinline__ static void mul2(uint32_t r[8], const uint32_t a[8], const uint32_t b[8],
+                                              const uint32_t c[8], const uint32_t d[8]) {
+    fe_mul2_shared(r, a, b, c, d, G1F{});
   }
 };
 
@@ -277,9 +286,8 @@ __device__ __forceinline__ void xyzz_mdbl(Xyzz& r, const Aff& q) {
   fe_dbl(t, s, f);
   fe_sub(r.x, r.x, t, f);
   fe_sub(t, s, r.x, f);
-  M::mul(r.y, m, t);
-  M::mul(t, w, q.y);
-  fe_sub(r.y, r.y, t, f);
+  fe_p_minus(u, q.y, f);
+  M::mul2(r.y, m, t, w, u);  // M (S - X3) - W y
   fe_copy(r.zz, v);
   fe_copy(r.zzz, w);
 }
@@ -306,9 +314,8 @@ __device__ __forceinline__ void xyzz_dbl(Xyzz& r, const Xyzz& p) {
   fe_dbl(t, s, f);
   fe_sub(x3, x3, t, f);
   fe_sub(t, s, x3, f);
-  M::mul(y3, m, t);
-  M::mul(t, w, p.y);
-  fe_sub(y3, y3, t, f);
+  fe_p_minus(u, p.y, f);
+  M::mul2(y3, m, t, w, u);  // M (S - X3) - W Y
   M::mul(r.zz, v, p.zz);
   M::mul(r.zzz, w, p.zzz);
   fe_copy(r.x, x3);
@@ -415,10 +422,9 @@ __device__ __forceinline__ void xyzz_add_affine(Xyzz& acc, const Aff& q) {
   fe_sub(t, t, ppp, f);
   fe_sub(t, t, qq, f);
   fe_sub(t, t, qq, f);        // X3
-  fe_sub(qq, qq, t, f);
-  M::mul(qq, r, qq);       // R (Q - X3)
-  M::mul(ppp, acc.y, ppp); // Y1 PPP
-  fe_sub(acc.y, qq, ppp, f);
+  fe_sub(qq, qq, t, f);        // Q - X3
+  fe_p_minus(acc.y, acc.y, f);  // -Y1 as p - Y1
+  M::mul2(acc.y, r, qq, acc.y, ppp);  // R (Q - X3) - Y1 PPP
   fe_copy(acc.x, t);
 }
 
@@ -464,10 +470,9 @@ __device__ __forceinline__ void xyzz_add(Xyzz& r, const Xyzz& p, const Xyzz& q) 
   fe_sub(t, t, ppp, f);
   fe_sub(t, t, qq, f);
   fe_sub(t, t, qq, f);        // X3
-  fe_sub(qq, qq, t, f);
-  M::mul(qq, rr, qq);
-  M::mul(s1, s1, ppp);
-  fe_sub(r.y, qq, s1, f);
+  fe_sub(qq, qq, t, f);        // Q - X3
+  fe_p_minus(s1, s1, f);       // -S1 as p - S1
+  M::mul2(r.y, rr, qq, s1, ppp);  // R (Q - X3) - S1 PPP
   fe_copy(r.x, t);
   fe_copy(r.zz, zz);
   fe_copy(r.zzz, zzz);

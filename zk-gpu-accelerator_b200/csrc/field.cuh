@@ -295,6 +295,67 @@ __device__ __forceinline__ void fe_mul(uint32_t r[8], const uint32_t a[8], const
   fe_copy(r, t);
 }
 
+// r = (a b + c d) * 2^-256 mod p, canonical, for a, b, c, d <= p. r may alias
+// any input.
+//
+// fe_mul's CIOS with two product rows per word i (t += a b_i, t += c d_i)
+// before the Montgomery row: one reduction for the sum of two products, so
+// 24 wide multiply-adds a word against 32 for two fe_mul calls and one
+// conditional subtraction instead of two. Bounds: with T < 2^256 before word
+// i, T + a b_i + c d_i + m p < 2^256 + 3 p 2^32 < 2^288 (word 8 never carries
+// out) and the shifted sum stays below T / 2^32 + a + c + p < 2^224 + 3p < 2^256
+// (p < 2^254); the final T = (ab + cd + M p) / 2^256 < 2p^2 / 2^256 + p < 2p.
+// The curve formulas take Y3 = R (Q - X3) - Y1 PPP as R (Q - X3) + (p - Y1) PPP
+// through it, the one place where two products are only summed.
+template <class F>
+__device__ __forceinline__ void fe_mul2(uint32_t r[8], const uint32_t a[8], const uint32_t b[8],
+                                        const uint32_t c[8], const uint32_t d[8], const F& f) {
+  uint32_t x[8], y[8], u[8], v[8], t[9];
+  fe_copy(x, a);
+  fe_copy(y, b);
+  fe_copy(u, c);
+  fe_copy(v, d);
+#pragma unroll
+  for (int j = 0; j < 9; ++j) t[j] = 0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    uint32_t lo[8], hi[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) split64((uint64_t)x[j] * y[i] + t[j], lo[j], hi[j]);
+    ZKB_ROW_CHAIN(t[1], t[2], t[3], t[4], t[5], t[6], t[7], t[8], t[8], lo, hi);
+    t[0] = lo[0];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) split64((uint64_t)u[j] * v[i] + t[j], lo[j], hi[j]);
+    ZKB_ROW_CHAIN(t[1], t[2], t[3], t[4], t[5], t[6], t[7], t[8], t[8], lo, hi);
+    t[0] = lo[0];
+    const uint32_t m = t[0] * f.ninv();
+#pragma unroll
+    for (int j = 0; j < 8; ++j) split64((uint64_t)m * f.p(j) + t[j], lo[j], hi[j]);
+    ZKB_ROW_CHAIN(t[0], t[1], t[2], t[3], t[4], t[5], t[6], t[7], t[8], lo, hi);
+    t[8] = 0;
+  }
+  fe_reduce_once(t, f);
+  fe_copy(r, t);
+}
+
+// r = p - a for a <= p: the negation as an operand of fe_mul2, in [0, p]
+// (a = 0 gives p, which fe_mul2 accepts). One borrow chain, no selection.
+template <class F>
+__device__ __forceinline__ void fe_p_minus(uint32_t r[8], const uint32_t a[8], const F& f) {
+  asm("sub.cc.u32 %0, %8, %16;\n\t"
+      "subc.cc.u32 %1, %9, %17;\n\t"
+      "subc.cc.u32 %2, %10, %18;\n\t"
+      "subc.cc.u32 %3, %11, %19;\n\t"
+      "subc.cc.u32 %4, %12, %20;\n\t"
+      "subc.cc.u32 %5, %13, %21;\n\t"
+      "subc.cc.u32 %6, %14, %22;\n\t"
+      "subc.u32 %7, %15, %23;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+      : "r"(f.p(0)), "r"(f.p(1)), "r"(f.p(2)), "r"(f.p(3)), "r"(f.p(4)), "r"(f.p(5)), "r"(f.p(6)),
+        "r"(f.p(7)), "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]),
+        "r"(a[7]));
+}
+
 // r = a^2 * 2^-256 mod p, canonical; r may alias a.
 //
 // SOS (separated operand scanning): the 512-bit square first, each
@@ -440,6 +501,30 @@ __device__ __forceinline__ void fe_mul_shared(uint32_t r[8], const uint32_t a[8]
 __device__ __forceinline__ void fe_mul_shared(uint32_t r[8], const uint32_t a[8],
                                               const uint32_t b[8], const FieldRT& f) {
   fe_mul(r, a, b, f);
+}
+
+template <class F>
+static __device__ __noinline__ Fe8 fe_mul2_outlined(const Fe8 a, const Fe8 b, const Fe8 c, const Fe8 d) {
+  Fe8 r;
+  fe_mul2(r.w, a.w, b.w, c.w, d.w, F{});
+  return r;
+}
+
+// the sum of two products' shared copy, as fe_mul_shared
+template <class F>
+__device__ __forceinline__ void fe_mul2_shared(uint32_t r[8], const uint32_t a[8], const uint32_t b[8],
+                                               const uint32_t c[8], const uint32_t d[8], const F&) {
+  Fe8 x, y, u, v;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    x.w[j] = a[j];
+    y.w[j] = b[j];
+    u.w[j] = c[j];
+    v.w[j] = d[j];
+  }
+  const Fe8 z = fe_mul2_outlined<F>(x, y, u, v);
+#pragma unroll
+  for (int j = 0; j < 8; ++j) r[j] = z.w[j];
 }
 
 // r = 2a, 3a, 4a, 8a mod p.
