@@ -334,8 +334,8 @@ int zkb_msm_fixed_batch(const zkb_msm_job* jobs, int count, void* workspace, siz
  * the workspace size queries): "msm.pairs_per_thread" (sorted pairs a bucket
  * thread adds in turn, 8..4096; default 0 = by size: the pair bound over 2^19,
  * as a power of two within 8..64),
- * "msm.slots_per_thread" (8), "msm.reduce_log_segment" (1: two-bucket
- * running-sum segments), "msm.sort" (1:
+ * "msm.slots_per_thread" (8), "msm.reduce_log_segment" (4: the
+ * first reduction level sums 16 buckets a lane, 512 a warp), "msm.sort" (1:
  * pairs grouped by a counting sort that skips zero digits; 0: a radix sort
  * of all pairs; the same points either way),
  * "ntt.max_log_radix" (log2 of the largest sub-transform one NTT pass does,

@@ -985,38 +985,85 @@ __global__ void __launch_bounds__(128) k_msm_acc_slots(const uint32_t* in_keys,
 // 4. window reduction
 // ---------------------------------------------------------------------------
 
-// One thread per (window, segment). X and U_in are [W][G_in]; outputs are
-// [W][G_in / L] (S scaled by L), or the window sums at the last level.
+// sum_b (b + 1) B_b per window, in levels. A level's items are pairs
+// (A_i, T_i): T_i is the sum of the buckets item i covers, scaled by D (the
+// buckets an item covers), and A_i their sum weighted 1, 2, ... from the
+// item's first bucket. Level 1's items are the buckets themselves (A = T = B,
+// D = 1). One warp takes a chunk of 32 L consecutive items of one window, L
+// per lane:
+//   lane t, items j = 0..L-1:  R_t = sum_j T_j,  V_t = sum_j A_j + sum_j j T_j
+//       (running sums from the top: two additions an item, three above level 1)
+//   chunk:  A = sum_t V_t + L sum_t t R_t,  T = 32 L sum_t R_t
+// and sum_t t R_t = sum_(t >= 1) SR_t with SR_t = sum_(u >= t) R_u, a suffix
+// scan across the lanes (five shuffled additions), then a tree sum of
+// Y_t = V_t + L SR_t (five more). The chunk's pair is the next level's item;
+// a level with one chunk per window writes the window sums. Per bucket that is
+// 2 + (11 + log2 L) / L XYZZ operations at level 1, and two or three levels
+// in all.
+__device__ __forceinline__ void shfl_down_xyzz(Xyzz& r, const Xyzz& a, int o) {
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    r.x[j] = __shfl_down_sync(0xffffffffu, a.x[j], o);
+    r.y[j] = __shfl_down_sync(0xffffffffu, a.y[j], o);
+    r.zz[j] = __shfl_down_sync(0xffffffffu, a.zz[j], o);
+    r.zzz[j] = __shfl_down_sync(0xffffffffu, a.zzz[j], o);
+  }
+}
+
+// A_in / T_in are [W][G_in] (T_in null at level 1: the buckets are both); a
+// warp per (window, chunk), chunks_per_window chunks of 32 << lL items. Out:
+// [W][chunks_per_window] pairs, or (T_out null) the window sums.
 template <class Mul>
-__global__ void __launch_bounds__(128) k_msm_reduce(const uint64_t* X, const uint64_t* U_in,
-                                                    int64_t G_in, int lL, int delta, int W,
-                                                    uint64_t* S_out, uint64_t* U_out,
-                                                    int final_level) {
-  const int64_t L = 1ll << lL;
-  const int64_t G_out = final_level ? 1 : G_in >> lL;
-  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (gid >= (int64_t)W * G_out) return;
-  const int64_t win = gid / G_out, t = gid % G_out;
-  const int64_t base = win * G_in + t * L;
-  const int64_t len = final_level ? G_in : L;
-  Xyzz running, tot, x;
-  xyzz_set_identity(running);
+__global__ void __launch_bounds__(128) k_msm_reduce(const uint64_t* A_in, const uint64_t* T_in,
+                                                    int64_t G_in, int lL, int64_t chunks_per_window,
+                                                    int64_t total_chunks, uint64_t* A_out,
+                                                    uint64_t* T_out) {
+  const int64_t chunk = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (chunk >= total_chunks) return;  // whole warps: the shuffles below see all 32 lanes
+  const int64_t win = chunk / chunks_per_window;
+  const int64_t c = chunk - win * chunks_per_window;
+  const int L = 1 << lL;
+  const int64_t first = (c * 32 + lane) * (int64_t)L;
+  const uint64_t* A = A_in + 16 * win * G_in;
+  const uint64_t* T = T_in ? T_in + 16 * win * G_in : nullptr;
+  Xyzz run, tot, x;
+  xyzz_set_identity(run);
   xyzz_set_identity(tot);
-  for (int64_t i = len - 1; i >= 0; --i) {
-    xyzz_load(x, X + 16 * (base + i));
-    xyzz_add<Mul>(running, running, x);
-    if (i > 0 || delta) xyzz_add<Mul>(tot, tot, running);
-  }
-  if (U_in) {
-    for (int64_t i = 0; i < len; ++i) {
-      xyzz_load(x, U_in + 16 * (base + i));
-      xyzz_add<Mul>(tot, tot, x);
+  for (int k = L - 1; k >= 0; --k) {
+    const int64_t i = first + k;
+    if (i < G_in) {
+      xyzz_load(x, (T ? T : A) + 16 * i);
+      xyzz_add<Mul>(run, run, x);
+      if (T) {
+        xyzz_load(x, A + 16 * i);
+        xyzz_add<Mul>(tot, tot, x);
+      }
     }
+    if (k > 0 || !T) xyzz_add<Mul>(tot, tot, run);  // level 1: weights 1..L, else 0..L-1 on T
   }
-  xyzz_store(U_out + 16 * (win * G_out + t), tot);
-  if (!final_level) {
-    for (int k = 0; k < lL; ++k) xyzz_dbl<Mul>(running, running);
-    xyzz_store(S_out + 16 * (win * G_out + t), running);
+  // run = R_t, tot = V_t. Suffix scan: run becomes SR_t.
+#pragma unroll 1
+  for (int o = 1; o < 32; o <<= 1) {
+    shfl_down_xyzz(x, run, o);
+    if (lane + o < 32) xyzz_add<Mul>(run, run, x);
+  }
+  if (lane > 0) {  // Y_t = V_t + L SR_t (lane 0 keeps SR_0, the chunk's total)
+    Xyzz sr = run;
+    for (int k = 0; k < lL; ++k) xyzz_dbl<Mul>(sr, sr);
+    xyzz_add<Mul>(tot, tot, sr);
+  }
+#pragma unroll 1
+  for (int o = 16; o > 0; o >>= 1) {
+    shfl_down_xyzz(x, tot, o);
+    if (lane < o) xyzz_add<Mul>(tot, tot, x);
+  }
+  if (lane == 0) {
+    xyzz_store(A_out + 16 * chunk, tot);
+    if (T_out) {
+      for (int k = 0; k < 5 + lL; ++k) xyzz_dbl<Mul>(run, run);
+      xyzz_store(T_out + 16 * chunk, run);
+    }
   }
 }
 
@@ -1115,7 +1162,7 @@ struct MsmPlan {
   int64_t nb = 0;  // buckets per window
   int k1 = 64;     // sorted pairs per bucket thread ("msm.pairs_per_thread", else by size)
   int k2 = 8;      // slots per merge thread ("msm.slots_per_thread")
-  int log_l = 1;   // log2 running-sum segment ("msm.reduce_log_segment")
+  int log_l = 4;   // log2 of the buckets a lane sums in reduction level 1 ("msm.reduce_log_segment")
   int call_products = 1;  // bucket kernels call one shared product ("msm.call_products")
   int counting_sort = 1;  // counting sort (1) or radix sort (0) of the pairs ("msm.sort")
   int table = 0;          // points are fixed-base tables: one bucket set per job
@@ -1450,28 +1497,28 @@ static int run_msm(const MsmJobs& J, const MsmPlan& p, char* ws, cudaStream_t s)
   uint64_t* wsum = reinterpret_cast<uint64_t*>(ws + p.off_wsum);
   {
     ProfSpan span("msm_reduce", s);
-    const uint64_t* X = buckets;
-    const uint64_t* U = nullptr;
-    int64_t G = p.nb;
-    int delta = 1, r = 0;
-    const int64_t L = 1ll << p.log_l;
-    while (G > L) {
-      const int64_t G_out = G / L;
-      const int64_t threads = windows * G_out;
-      auto red = p.call_products ? k_msm_reduce<CallMul> : k_msm_reduce<InlineMul>;
-      red<<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(X, U, G, p.log_l, delta,
-                                                                     (int)windows, rs[r], ru[r], 0);
-      ZKB_TRY(check_launch("msm window reduction"));
-      X = rs[r];
-      U = ru[r];
-      r ^= 1;
-      G = G_out;
-      delta = 0;
-    }
     auto red = p.call_products ? k_msm_reduce<CallMul> : k_msm_reduce<InlineMul>;
-    red<<<(unsigned)((windows + 127) / 128), 128, 0, s>>>(X, U, G, p.log_l, delta,
-                                                                   (int)windows, nullptr, wsum, 1);
-    ZKB_TRY(check_launch("msm window sums"));
+    const uint64_t* A = buckets;
+    const uint64_t* T = nullptr;
+    int64_t G = p.nb;
+    int lL = p.log_l, r = 0;
+    for (;;) {
+      const int64_t per = (int64_t)32 << lL;
+      const int64_t chunks = (G + per - 1) / per;
+      const bool last = chunks == 1;
+      const int64_t total = windows * chunks;
+      red<<<(unsigned)((total * 32 + 127) / 128), 128, 0, s>>>(A, T, G, lL, chunks, total,
+                                                                last ? wsum : rs[r], last ? nullptr : ru[r]);
+      ZKB_TRY(check_launch(last ? "msm window sums" : "msm window reduction"));
+      if (last) break;
+      A = rs[r];
+      T = ru[r];
+      r ^= 1;
+      G = chunks;
+      // the next level: the fewest items a lane that finish the window, at most 16
+      lL = 0;
+      while (lL < 4 && ((int64_t)32 << lL) < G) ++lL;
+    }
   }
 
   // 5. finalize
