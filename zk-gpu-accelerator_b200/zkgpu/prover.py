@@ -144,11 +144,18 @@ class ProofJob:
 
     def upload(self) -> None:
         """Pinned host rows to the device, then A, B, C into Montgomery form (current stream)."""
-        m = self.m
+        self.copy_rows()
+        self.to_montgomery()
+
+    def copy_rows(self) -> None:
+        """The pinned host rows (a, b, c, z, 1 / Z_H(g)) to the device (current stream)."""
         self.plain.copy_(self.host, non_blocking=True)
+
+    def to_montgomery(self) -> None:
+        """A, B, C into Montgomery form (current stream, after copy_rows)."""
         f = BN254_FR._field()
         _native.check(_native.lib().zkb_field_to_mont(ctypes.byref(f), _native.ptr(self.plain),
-                                                       _native.ptr(self.abc), 3 * m, _native.stream_ptr()),
+                                                       _native.ptr(self.abc), 3 * self.m, _native.stream_ptr()),
                       "zkb_field_to_mont")
 
     def witness_rows(self) -> Any:

@@ -27,9 +27,11 @@ The service
 - reports each job's latency (arrival to the device-side completion of its
   last MSM) and the throughput.
 
-Stages (one per tick): INTT (upload + 3 inverse NTTs; A, B, L MSMs start)
--> COSET (3 coset NTTs) -> QUOTIENT (pointwise + inverse coset NTT + h to
-plain form) -> MSM (the H MSM) -> done when both MSM batches completed.
+Stages (one per tick): INTT (host rows copied on a stream of their own,
+while the tick's other transforms and the MSM batches run; 3 inverse NTTs;
+A, B, L MSMs start once the witness is on the device) -> COSET (3 coset NTTs)
+-> QUOTIENT (pointwise + inverse coset NTT + h to plain form) -> MSM (the H
+MSM) -> done when both MSM batches completed.
 
 Scheduler holds the policy and needs no GPU (tested on the CPU with a fake
 clock); Server drives it on the device.
@@ -182,24 +184,27 @@ class Server:
                   first)
     table       : optional FixedBaseTable built from `bases`: the MSM batches then
                   run over it (zkb_msm_fixed_batch), with the same results
+    max_in_flight : jobs admitted at once at most (the HBM budget may admit fewer)
     """
 
     def __init__(self, bases: Any, hbm_budget: int, max_ticks_ahead: int = 2, msm_streams: int = 2,
                  msm_priority: str = "high", tick_priority: str = "normal",
-                 max_batch_points: int = 1 << 22, table: Any = None) -> None:
+                 max_batch_points: int = 1 << 22, table: Any = None, max_in_flight: int = 256) -> None:
         torch = _native.require_cuda()
         self.torch = torch
         self.bases = bases
         self.table = table
-        self.sched = Scheduler(hbm_budget)
+        self.sched = Scheduler(hbm_budget, max_in_flight)
         self.max_ticks_ahead = max_ticks_ahead
         lo, hi = torch.cuda.Stream.priority_range()
         level = {"high": hi, "normal": 0, "low": lo}
-        self.main = torch.cuda.Stream(priority=level[tick_priority])
+        self.main = _stream("ticks", level[tick_priority])
+        # admitted jobs' host rows go up on their own stream, beside the ticks and the MSMs
+        self.copy_stream = _stream("copies", 0)
         # MSM streams pull the pending MSM work whenever their last batch is done; two let
         # one batch's latency-bound tail (bucket reduction, final combination) overlap the
         # next batch's accumulation
-        self.msm_streams = [torch.cuda.Stream(priority=level[msm_priority]) for _ in range(max(1, msm_streams))]
+        self.msm_streams = [_stream(f"msm{k}", level[msm_priority]) for k in range(max(1, msm_streams))]
         self.msm_last: list[Any] = [None] * len(self.msm_streams)
         self.pending_msm: list[tuple[list, list[int], Any]] = []
         self.msm_batches = 0
@@ -257,7 +262,7 @@ class Server:
                 now = clock() - t0
                 admitted = self.sched.admit(now)
                 for job_id in admitted:
-                    self.jobs[job_id] = ProofJob(self.pending.pop(job_id), self.bases, job_id)
+                    self.jobs[job_id] = self._new_job(self.pending.pop(job_id), job_id)
                     self.records[job_id].admitted_s = now
                     self.outstanding[job_id] = 0
                 tick = self.sched.next_tick(admitted)
@@ -278,6 +283,20 @@ class Server:
                     self._collect(block=False)
         torch.cuda.synchronize()
         return [self.records[k] for k in range(len(requests))]
+
+    def _new_job(self, request: ProofRequest, job_id: int) -> ProofJob:
+        """A job's buffers, from the copy stream's share of the allocator: its rows are written
+        on that stream first, so the memory handed to it is never memory that work queued on
+        another stream may still use (a block freed on the tick stream while a queued
+        transform still reads it would be, if the job were allocated there). The streams that
+        use the buffers later are recorded, so the block is reused only after their work."""
+        torch = self.torch
+        with torch.cuda.stream(self.copy_stream):
+            job = ProofJob(request, self.bases, job_id)
+        job._mem.record_stream(self.main)
+        for stream in self.msm_streams:
+            job._mem.record_stream(stream)
+        return job
 
     def _collect(self, block: bool) -> None:
         """Retire jobs whose MSM batches all finished; completion time from the device clock."""
@@ -357,19 +376,53 @@ class Server:
         before = int(lib.zkb_launch_count())
         s = _native.stream_ptr()
         f = ctypes.byref(_native_fr())
-        for job_id in tick.admitted:
-            self.jobs[job_id].upload()
-        upload_event = None
+        # The admitted jobs' rows go up in groups (as many jobs as one transform launch
+        # holds), each with its own event: the copies land while this tick's transforms of
+        # resident jobs and the MSM batches run, and a group's own work starts as soon as
+        # its rows are on the device, while the next group's copies are still running.
+        groups = []
+        per = max(1, MAX_NTT_PER_LAUNCH // 3)
         if tick.admitted:
-            upload_event = torch.cuda.Event()
-            upload_event.record(self.main)
+            with torch.cuda.stream(self.copy_stream):
+                for lo in range(0, len(tick.admitted), per):
+                    ids = tick.admitted[lo : lo + per]
+                    for job_id in ids:
+                        self.jobs[job_id].copy_rows()
+                    event = torch.cuda.Event()
+                    event.record(self.copy_stream)
+                    groups.append((ids, event))
         for job_id in tick.quotient:
             _native.check(lib.zkb_quotient_pointwise(*self.jobs[job_id].quotient_args(), s),
                           "zkb_quotient_pointwise")
-        entries = []
-        for stage, ids in ((STAGE_INTT, tick.intt), (STAGE_COSET, tick.coset), (STAGE_QUOTIENT, tick.quotient)):
+        resident = []
+        for stage, ids in ((STAGE_COSET, tick.coset), (STAGE_QUOTIENT, tick.quotient)):
             for job_id in ids:
-                entries.extend(self.jobs[job_id].ntt_entries(stage))
+                resident.extend(self.jobs[job_id].ntt_entries(stage))
+        self._ntt_batches(resident, f, s)
+        for job_id in tick.quotient:
+            self.jobs[job_id].h_to_plain()
+        for ids, event in groups:  # the admitted jobs are the tick's INTT stage
+            self.main.wait_event(event)
+            for job_id in ids:
+                self.jobs[job_id].to_montgomery()
+            self._ntt_batches([e for j in ids for e in self.jobs[j].ntt_entries(STAGE_INTT)], f, s)
+        prev_event = self.prev_tick_event
+        tick_event = torch.cuda.Event()
+        tick_event.record(self.main)
+        self.tick_events.append(tick_event)
+        self.prev_tick_event = tick_event
+        for ids, event in groups:
+            # A, B and L need only the witness: they start once it is copied, beside the quotient
+            self._queue_msm([e for j in ids for e in self.jobs[j].msm_entries()[:3]], ids, event)
+        if tick.msm:
+            # H needs h, written by the previous tick
+            self._queue_msm([self.jobs[j].msm_entries()[3] for j in tick.msm], tick.msm, prev_event)
+        self.ticks += 1
+        self.launches += int(lib.zkb_launch_count()) - before
+
+    def _ntt_batches(self, entries: list, f: Any, s: int) -> None:
+        """Transforms (in, out, n, invert, coset) as zkb_ntt_batch launches of up to 64."""
+        lib = _native.lib()
         for lo in range(0, len(entries), MAX_NTT_PER_LAUNCH):
             chunk = entries[lo : lo + MAX_NTT_PER_LAUNCH]
             jobs = (_native.ZkbNttJob * len(chunk))()
@@ -382,22 +435,23 @@ class Server:
             ws = _native.workspace(ws_bytes)
             _native.check(lib.zkb_ntt_batch(f, jobs, len(chunk), _native.ptr(ws), ws_bytes, None, s),
                           "zkb_ntt_batch")
-        for job_id in tick.quotient:
-            self.jobs[job_id].h_to_plain()
-        prev_event = self.prev_tick_event
-        tick_event = torch.cuda.Event()
-        tick_event.record(self.main)
-        self.tick_events.append(tick_event)
-        self.prev_tick_event = tick_event
-        if tick.admitted:
-            # A, B and L need only the witness: they start at admission, beside the quotient
-            self._queue_msm([e for j in tick.admitted for e in self.jobs[j].msm_entries()[:3]],
-                            tick.admitted, upload_event)
-        if tick.msm:
-            # H needs h, written by the previous tick
-            self._queue_msm([self.jobs[j].msm_entries()[3] for j in tick.msm], tick.msm, prev_event)
-        self.ticks += 1
-        self.launches += int(lib.zkb_launch_count()) - before
+
+
+_STREAMS: dict[tuple[int, str, int], Any] = {}
+
+
+def _stream(role: str, priority: int) -> Any:
+    """The process's one stream for a role and priority on the current device. Servers reuse
+    them: torch's caching allocator hands a freed block out again only on the stream it was
+    allocated on, so a server with new streams could use none of the memory its predecessors
+    cached, and each run grew the reserved memory (by ~29 GB for 200 queued jobs) until an
+    allocation failed and the allocator released its cache behind a full device
+    synchronisation."""
+    torch = _native.torch_module()
+    key = (torch.cuda.current_device(), role, priority)
+    if key not in _STREAMS:
+        _STREAMS[key] = torch.cuda.Stream(priority=priority)
+    return _STREAMS[key]
 
 
 def _native_fr() -> Any:
