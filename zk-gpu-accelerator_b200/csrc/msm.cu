@@ -1856,9 +1856,9 @@ int zkb_msm_no_alloc(const uint64_t* points, const uint64_t* scalars, int64_t n,
   const int w = window_size ? window_size : default_window(n);
   MsmPlan p;
   ZKB_TRY(make_plan(&n, 1, w, p));
-  // short bucket chains and two-bucket reduction segments, which suit small
+  // short bucket chains and short first-level reduction runs, which suit small
   // MSMs, take more scratch: when the plan does not fit the fixed scratch, the
-  // compact shape (at least 64 pairs per thread, 4-bucket segments) may
+  // compact shape (at least 64 pairs per thread, at least 4 buckets a lane) may
   if (p.total > kNoAllocScratchBytes && (p.k1 < 64 || p.log_l < 2)) {
     ZKB_TRY(make_plan(&n, 1, w, p, 0, p.k1 > 64 ? p.k1 : 64, p.log_l > 2 ? p.log_l : 2));
   }
