@@ -1122,14 +1122,19 @@ def run_served(n_jobs: int = 2000, rate: float = 200.0, log_max: int = 20, seed:
         torch.cuda.synchronize()
     plain_s = time.perf_counter() - t0
     budget = 60 << 30
-    Server(bases, budget, table=table).run(sample[:10], [0.0] * 10)  # warm-up: tables, allocator
-    # capacity first: the first 200 jobs all queued at once (closed loop). It also grows the
-    # allocator's pool to the largest number of jobs in flight, so the timed stream below
-    # does not stop for device allocations, which can synchronise the device.
-    cap = Server(bases, budget, table=table)
-    t0 = time.perf_counter()
-    cap_recs = cap.run(reqs[:200], [0.0] * min(200, n_jobs))
-    cap_s = summarize(cap_recs, time.perf_counter() - t0)
+    # warm-up: the first 200 jobs queued at once, untimed. It builds the tables and grows the
+    # allocator's pool (on the servers' streams, which every Server shares) to the largest
+    # number of jobs in flight, so no timed run below stops for device allocations.
+    n_cap = min(200, n_jobs)
+    Server(bases, budget, table=table).run(reqs[:n_cap], [0.0] * n_cap)
+    # capacity: the same 200 jobs queued at once (closed loop), twice; the mean of the two
+    cap_rates = []
+    for _ in range(2):
+        cap = Server(bases, budget, table=table)
+        t0 = time.perf_counter()
+        cap_recs = cap.run(reqs[:n_cap], [0.0] * n_cap)
+        cap_rates.append(summarize(cap_recs, time.perf_counter() - t0)["jobs_per_s"])
+    cap_s = {"jobs_per_s": sum(cap_rates) / len(cap_rates)}
     # the same Poisson stream served `runs` times: the line's latencies are the median run's,
     # with every run's p50 / p99 beside them for the run-to-run spread
     summaries = []
@@ -1153,8 +1158,9 @@ def run_served(n_jobs: int = 2000, rate: float = 200.0, log_max: int = 20, seed:
         "plain_jobs_per_s": round(plain_jobs_s, 1),
         "speedup_vs_plain": round(s["jobs_per_s"] / plain_jobs_s, 3),
         "capacity_jobs_per_s": round(cap_s["jobs_per_s"], 1),
+        "capacity_runs_jobs_per_s": [round(x, 1) for x in cap_rates],
         "capacity_vs_plain": round(cap_s["jobs_per_s"] / plain_jobs_s, 3),
-        "capacity": "the first 200 jobs queued at once (closed loop), same server",
+        "capacity": "the first 200 jobs queued at once (closed loop): the mean of two runs after one untimed run",
         "plain": f"the first {len(sample)} jobs one at a time (one call per NTT / MSM, synchronised per job)",
         "ticks": srv.ticks, "gpu_launches": srv.launches, "hbm_budget_bytes": budget,
         "latency": "arrival (host clock) to the device-side completion of the job's last MSM batch",
