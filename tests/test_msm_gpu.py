@@ -309,3 +309,45 @@ def test_affine_rounds_with_inlined_products():
     sc = gen(case["scalar_seed"], n)
     knobs = {"msm.affine_rounds": 2, "msm.affine_batch": 32, "msm.call_products": 0}
     assert _with_knobs(knobs, lambda: msm_pippenger_rows(bases, sc)) == expected_point(case)
+
+
+# ------------------------------------------------------------------
+# Bucket reduction by warps ("msm.reduce_log_segment": buckets a lane sums at level 1)
+# ------------------------------------------------------------------
+
+
+@pytest.mark.parametrize("log_l", [0, 1, 2, 3, 4, 5, 8])
+@pytest.mark.parametrize("case", golden("msm.json")["seeded"], ids=lambda c: f"{c['kind']}-{c['n']}")
+def test_every_reduction_segment_gives_the_references_points(case, log_l):
+    """Every segment length of the first reduction level (1..256 buckets a lane), at windows
+    whose buckets take one level (w <= 5 at 16 a lane), two, and three (w = 20: 2^19
+    buckets, 1,024 chunks at level 2), against the reference's points."""
+    import torch
+
+    n = case["n"]
+    bases = _bases(n, case["base_seed"])
+    gen = wl.uniform_fr if case["kind"] == "uniform" else wl.skewed_scalars
+    sc = gen(case["scalar_seed"], n)
+    sc_dev = torch.from_numpy(sc).cuda()
+    knobs = {"msm.reduce_log_segment": log_l}
+    for w in (None, 1, 5, 11, 16):
+        assert _with_knobs(knobs, lambda: msm_pippenger_rows(bases, sc, window_size=w)) == expected_point(case), w
+    assert _with_knobs(knobs, lambda: _msm_raw(bases, sc_dev, n, 20)) == expected_point(case)
+
+
+def test_reduction_segments_in_batches_and_fixed_base_tables():
+    """The batch and fixed-base forms (one bucket set per job) at segment lengths 1, 16, 256,
+    against each job alone at the default knobs."""
+    from zkgpu import batch
+
+    n = 3000
+    bases = _bases(n, 71)
+    scs = [wl.uniform_fr(72, n), wl.skewed_scalars(73, 1777), wl.uniform_fr(74, 5)]
+    alone = [msm_pippenger_rows(bases[: s.shape[0]], s) for s in scs]
+    table = msm_gpu.FixedBaseTable(bases, 12)
+    for log_l in (0, 4, 8):
+        knobs = {"msm.reduce_log_segment": log_l}
+        got = _with_knobs(knobs, lambda: batch.msm_batch([bases[: s.shape[0]] for s in scs], scs))
+        assert got == alone, log_l
+        got_t = _with_knobs(knobs, lambda: batch.msm_fixed_batch(table, scs))
+        assert got_t == alone, log_l
