@@ -580,13 +580,20 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     if not args.skip_e2e:
         e2e = _run_e2e(args, step, dist, device, log_msm, log_ntt)
 
+    # Each leg below starts from an allocator holding no cached blocks of the legs before it:
+    # torch keeps freed blocks per stream, and a leg that allocates on its own streams cannot
+    # reuse them, so the cache of earlier legs would only push it into failed allocations and
+    # the full synchronisations that release the cache (outside every timed region).
     batched = served = None
     if args.workload == "large" and not args.skip_batched:
+        release_cached_memory()
         batched = run_batched()
     if args.workload == "large" and not args.skip_served:
+        release_cached_memory()
         served = run_served()
     int64 = None
     if args.workload == "large" and not args.skip_int64:
+        release_cached_memory()
         int64 = run_int64(cpu=rank == 0 and not args.skip_cpu_baseline)
 
     sharded = None
@@ -657,6 +664,17 @@ def _profile_traffic(kernel: str, n: int) -> float | None:
         return round(found[float(n)])
     points = max(found)
     return round(found[points] * n / points)
+
+
+def release_cached_memory() -> None:
+    """Return the caching allocator's free blocks to the device (between legs, untimed)."""
+    import gc
+
+    import torch
+
+    gc.collect()
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
 
 
 def _run_e2e(args, step: Step, dist, device, log_msm: int, log_ntt: int) -> dict:

@@ -333,8 +333,10 @@ int zkb_msm_fixed_batch(const zkb_msm_job* jobs, int count, void* workspace, siz
 /* Tuning knobs, read by each call when it plans its work (so they also change
  * the workspace size queries): "msm.pairs_per_thread" (sorted pairs a bucket
  * thread adds in turn, 8..4096; default 0 = by size: the pair bound over 2^19,
- * as a power of two within 8..64),
- * "msm.slots_per_thread" (8), "msm.reduce_log_segment" (4: the
+ * as a power of two within 8..64, or within 8..16 for zkb_msm and
+ * zkb_msm_no_alloc), "msm.call_pairs_cap" (16: that upper limit for the
+ * one-MSM calls, 8..64; shorter bucket blocks let work on other streams reach
+ * the SMs sooner), "msm.slots_per_thread" (8), "msm.reduce_log_segment" (4: the
  * first reduction level sums 16 buckets a lane, 512 a warp), "msm.sort" (1:
  * pairs grouped by a counting sort that skips zero digits; 0: a radix sort
  * of all pairs; the same points either way),

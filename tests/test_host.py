@@ -93,7 +93,7 @@ def test_host_only_queries():
 
 
 def test_tuning_knobs_validate_and_plan_the_workspace():
-    defaults = {"msm.pairs_per_thread": 0, "msm.slots_per_thread": 8, "msm.reduce_log_segment": 4, "msm.sort": 1,
+    defaults = {"msm.pairs_per_thread": 0, "msm.slots_per_thread": 8, "msm.reduce_log_segment": 4, "msm.call_pairs_cap": 16, "msm.sort": 1,
                 "ntt.max_log_radix": 0, "ntt.cta_log_elems": 0, "ntt.threads": 0, "ntt.full_table_mb": 4096,
                 "ntt64.first_col_log": -1, "ntt64.first_max_k": 0, "ntt64.col_log": 0, "ntt64.max_k": 0}
     assert {k: _native.tune_get(k) for k in defaults} == defaults

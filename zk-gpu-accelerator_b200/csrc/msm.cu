@@ -1190,9 +1190,18 @@ static int64_t aff_blocks(int64_t entries, int k) {
   return std::max<int64_t>(1, std::min<int64_t>((entries + per - 1) / per, 2 * 148));
 }
 
+// The longest automatic run of sorted pairs a bucket thread takes in a one-MSM
+// call ("msm.call_pairs_cap", default 16; batches go up to 64). A bucket block
+// then lasts about 0.5 ms instead of 2 ms at 2^22 points, so kernels the caller
+// runs beside the MSM on other streams (a transform of higher priority) wait at
+// most that long for an SM at each of their launches. Measured on B200, the
+// bench's end-to-end step (two one-call MSMs beside two transforms and their
+// copies): 47.3 to 44.3 ms; the one-call MSM 2^22 alone 18.06 to 18.29 ms.
+static int single_call_pairs_cap() { return tune_get("msm.call_pairs_cap"); }
+
 // Plan for a batch of jobs with point counts sizes[0..count) at window w.
 static int make_plan(const int64_t* sizes, int count, int w, MsmPlan& p, int table = 0, int k1 = 0,
-                     int log_l = 0) {
+                     int log_l = 0, int k1_cap = 64) {
   p.count = count;
   p.first.assign(count + 1, 0);
   for (int j = 0; j < count; ++j) p.first[j + 1] = p.first[j] + sizes[j];
@@ -1241,7 +1250,7 @@ static int make_plan(const int64_t* sizes, int count, int w, MsmPlan& p, int tab
   p.k1 = k1 > 0 ? k1 : tune_get("msm.pairs_per_thread");
   if (p.k1 < 8) {
     p.k1 = 8;
-    while (p.k1 < 64 && ((int64_t)p.k1 << 20) <= p.E_list) p.k1 <<= 1;
+    while (p.k1 < k1_cap && ((int64_t)p.k1 << 20) <= p.E_list) p.k1 <<= 1;
   }
   p.k2 = tune_get("msm.slots_per_thread");
   p.log_l = log_l > 0 ? log_l : tune_get("msm.reduce_log_segment");
@@ -1635,7 +1644,7 @@ size_t zkb_msm_workspace_bytes(int64_t n, int window_size) {
   const int w = window_size ? window_size : default_window(n);
   if (w < 1 || w > kMsmMaxWindow) return 0;
   MsmPlan p;
-  if (make_plan(&n, 1, w, p) != ZKB_OK) return 0;
+  if (make_plan(&n, 1, w, p, 0, 0, 0, single_call_pairs_cap()) != ZKB_OK) return 0;
   return p.total;
 }
 
@@ -1661,7 +1670,7 @@ int zkb_msm(const uint64_t* points, const uint64_t* scalars, int64_t n, int wind
   ZKB_TRY(check_align(workspace, 256, "workspace"));
   const int w = window_size ? window_size : default_window(n);
   MsmPlan p;
-  ZKB_TRY(make_plan(&n, 1, w, p));
+  ZKB_TRY(make_plan(&n, 1, w, p, 0, 0, 0, single_call_pairs_cap()));
   if ((int64_t)p.E >= (1ll << 31)) {
     return fail(ZKB_EINVAL, "%lld points at window %d exceed the sort's 2^31 pairs",
                 (long long)n, w);
@@ -1855,7 +1864,7 @@ int zkb_msm_no_alloc(const uint64_t* points, const uint64_t* scalars, int64_t n,
   ZKB_TRY(check_align(scalars, 16, "scalars"));
   const int w = window_size ? window_size : default_window(n);
   MsmPlan p;
-  ZKB_TRY(make_plan(&n, 1, w, p));
+  ZKB_TRY(make_plan(&n, 1, w, p, 0, 0, 0, single_call_pairs_cap()));
   // short bucket chains and short first-level reduction runs, which suit small
   // MSMs, take more scratch: when the plan does not fit the fixed scratch, the
   // compact shape (at least 64 pairs per thread, at least 4 buckets a lane) may

@@ -25,6 +25,7 @@ static Knob g_knobs[] = {
     {"msm.pairs_per_thread", 0, 0, 4096},    // sorted pairs each bucket thread adds (8..4096; 0 = by size)
     {"msm.slots_per_thread", 8, 4, 4096},    // partial sums each merge thread adds
     {"msm.reduce_log_segment", 4, 0, 8},     // log2 of the buckets a lane sums in the first reduction level
+    {"msm.call_pairs_cap", 16, 8, 64},       // longest automatic bucket run of a one-MSM call
     {"msm.call_products", 1, 0, 1},          // bucket kernels call one shared product (1) or inline all (0)
     {"msm.sort", 1, 0, 1},                   // pairs grouped by a counting sort (1) or a radix sort (0)
     {"msm.affine_rounds", 0, -1, 8},         // affine rounds before the XYZZ levels (0 = none, -1 = by size)
