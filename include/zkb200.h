@@ -358,7 +358,10 @@ int zkb_msm_fixed_batch(const zkb_msm_job* jobs, int count, void* workspace, siz
  * 0: the per-thread gather form; the same rows either way), "ntt.tma_grid"
  * (1: one tile per block; 0: one persistent wave of double-buffered blocks),
  * "ntt.tma_blocks_per_sm" (0, or 5 / 6: the pass kernel of 128-thread blocks
- * with its registers capped for that many blocks per SM);
+ * with its registers capped for that many blocks per SM), "ntt.lazy" (1:
+ * inside a TMA pass, values stay in [0, 2p) between butterfly rounds and are
+ * made canonical at the store, for moduli below 2^254; 0: canonical after
+ * every operation; the same rows either way);
  * "msm.affine_rounds" (rounds in which every bucket's list is halved by affine
  * additions sharing one inversion per block, before the XYZZ levels; 0 = none,
  * the default; -1 = by size; 1..8 forced), "msm.affine_batch" (output entries

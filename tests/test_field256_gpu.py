@@ -329,6 +329,42 @@ def test_tma_passes_equal_gather_passes_at_every_size(cta_log):
     assert lib.zkb_ntt_wait_timeouts() == before == 0
 
 
+@pytest.mark.parametrize("cta_log", [9, 12])
+def test_lazy_reduction_passes_give_the_same_rows(cta_log):
+    """TMA passes with values in [0, 2p) between rounds ("ntt.lazy" = 1) give the canonical
+    passes' rows for every size 2^2..2^22, forward / inverse / coset, at both tile sizes; and at
+    2^20 the rows of the C port. Inputs include 0, 1 and p - 1 (the values the lazy ranges'
+    edges are made of)."""
+    from zkgpu import _native
+
+    lib = _native.lib()
+    saved = _native.tune_get("ntt.lazy")
+    try:
+        _native.tune_set("ntt.cta_log_elems", cta_log)
+        for log_n in range(2, 23):
+            n = 1 << log_n
+            plain = wl.uniform_fr(400 + log_n, n)
+            plain[0] = (0, 0, 0, 0)
+            plain[n // 2] = _native.limbs(R - 1)
+            plain[n - 1] = (1, 0, 0, 0)
+            rows = BN254_FR.to_montgomery(plain)
+            for invert, coset in ((False, None), (True, None), (False, 5), (True, 7)):
+                _native.tune_set("ntt.lazy", 1)
+                got = BN254_FR.ntt(rows, invert=invert, coset=coset)
+                _native.tune_set("ntt.lazy", 0)
+                want = BN254_FR.ntt(rows, invert=invert, coset=coset)
+                assert bool((got == want).all()), (log_n, invert, coset)
+        n = 1 << 20
+        plain = wl.uniform_fr(499, n)
+        _native.tune_set("ntt.lazy", 1)
+        got = BN254_FR.ntt(BN254_FR.to_montgomery(plain), coset=5)
+        assert np.array_equal(got.cpu().numpy(), co.ntt(co.to_mont(co.FR, plain), coset=5, threads=os.cpu_count() or 1))
+    finally:
+        _native.tune_set("ntt.lazy", saved)
+        _native.tune_set("ntt.cta_log_elems", 0)
+    assert lib.zkb_ntt_wait_timeouts() == 0
+
+
 def test_ntt_2_24_config_size():
     """Config 3's NTT: 2^24 elements (512 MiB), plain and coset g = 5, against the C oracle,
     plus the size-independent round trips."""

@@ -587,7 +587,114 @@ __device__ __forceinline__ void plane_store(uint4* lo, uint4* hi, int i, const u
   hi[i] = make_uint4(x[4], x[5], x[6], x[7]);
 }
 
-template <class F, int kThreads = kNttThreads, int kMinBlocks = 1>
+// ---- lazy reduction inside a pass (moduli below 2^254) ----------------------
+// Between the butterfly rounds of a pass, values may lie anywhere in [0, 2p)
+// instead of [0, p): a difference becomes a - b + 2p, in (0, 4p), with no
+// test, when a product by a canonical twiddle follows, and a product drops its
+// last conditional subtraction. Both stay exact because 4p < 2^256: the sum of
+// two values below 2p never carries out, and CIOS on a < 4p, b < p ends below
+// (4p^2 + 2^256 p) / 2^256 < 2p. Values are canonical again before a pass stores
+// them.
+
+// 2p, word j (p < 2^254, so 2p fits eight words)
+template <class F>
+__device__ __forceinline__ uint32_t two_p(const F& f, int j) {
+  return (f.p(j) << 1) | (j ? f.p(j - 1) >> 31 : 0u);
+}
+
+// r = a + b, then - 2p if that is at least 2p: [0, 2p) for a, b < 2p.
+template <class F>
+__device__ __forceinline__ void lz_add(uint32_t r[8], const uint32_t a[8], const uint32_t b[8], const F& f) {
+  uint32_t s[8], d[8], bw;
+  asm("add.cc.u32 %0, %8, %16;\n\t"
+      "addc.cc.u32 %1, %9, %17;\n\t"
+      "addc.cc.u32 %2, %10, %18;\n\t"
+      "addc.cc.u32 %3, %11, %19;\n\t"
+      "addc.cc.u32 %4, %12, %20;\n\t"
+      "addc.cc.u32 %5, %13, %21;\n\t"
+      "addc.cc.u32 %6, %14, %22;\n\t"
+      "addc.u32 %7, %15, %23;"
+      : "=r"(s[0]), "=r"(s[1]), "=r"(s[2]), "=r"(s[3]), "=r"(s[4]), "=r"(s[5]), "=r"(s[6]), "=r"(s[7])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]),
+        "r"(b[0]), "r"(b[1]), "r"(b[2]), "r"(b[3]), "r"(b[4]), "r"(b[5]), "r"(b[6]), "r"(b[7]));
+  asm("sub.cc.u32 %0, %9, %17;\n\t"
+      "subc.cc.u32 %1, %10, %18;\n\t"
+      "subc.cc.u32 %2, %11, %19;\n\t"
+      "subc.cc.u32 %3, %12, %20;\n\t"
+      "subc.cc.u32 %4, %13, %21;\n\t"
+      "subc.cc.u32 %5, %14, %22;\n\t"
+      "subc.cc.u32 %6, %15, %23;\n\t"
+      "subc.cc.u32 %7, %16, %24;\n\t"
+      "subc.u32 %8, 0, 0;"
+      : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]), "=r"(bw)
+      : "r"(s[0]), "r"(s[1]), "r"(s[2]), "r"(s[3]), "r"(s[4]), "r"(s[5]), "r"(s[6]), "r"(s[7]),
+        "r"(two_p(f, 0)), "r"(two_p(f, 1)), "r"(two_p(f, 2)), "r"(two_p(f, 3)), "r"(two_p(f, 4)),
+        "r"(two_p(f, 5)), "r"(two_p(f, 6)), "r"(two_p(f, 7)));
+#pragma unroll
+  for (int j = 0; j < 8; ++j) r[j] = bw ? s[j] : d[j];
+}
+
+// r = a - b + 2p in (0, 4p) for a, b < 2p: an operand of lz_mul only.
+template <class F>
+__device__ __forceinline__ void lz_sub_open(uint32_t r[8], const uint32_t a[8], const uint32_t b[8], const F& f) {
+  uint32_t d[8];
+  asm("sub.cc.u32 %0, %8, %16;\n\t"
+      "subc.cc.u32 %1, %9, %17;\n\t"
+      "subc.cc.u32 %2, %10, %18;\n\t"
+      "subc.cc.u32 %3, %11, %19;\n\t"
+      "subc.cc.u32 %4, %12, %20;\n\t"
+      "subc.cc.u32 %5, %13, %21;\n\t"
+      "subc.cc.u32 %6, %14, %22;\n\t"
+      "subc.u32 %7, %15, %23;"
+      : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]),
+        "r"(b[0]), "r"(b[1]), "r"(b[2]), "r"(b[3]), "r"(b[4]), "r"(b[5]), "r"(b[6]), "r"(b[7]));
+  // modulo 2^256 the wrapped difference plus 2p is the exact a - b + 2p
+  asm("add.cc.u32 %0, %0, %8;\n\t"
+      "addc.cc.u32 %1, %1, %9;\n\t"
+      "addc.cc.u32 %2, %2, %10;\n\t"
+      "addc.cc.u32 %3, %3, %11;\n\t"
+      "addc.cc.u32 %4, %4, %12;\n\t"
+      "addc.cc.u32 %5, %5, %13;\n\t"
+      "addc.cc.u32 %6, %6, %14;\n\t"
+      "addc.u32 %7, %7, %15;"
+      : "+r"(d[0]), "+r"(d[1]), "+r"(d[2]), "+r"(d[3]), "+r"(d[4]), "+r"(d[5]), "+r"(d[6]), "+r"(d[7])
+      : "r"(two_p(f, 0)), "r"(two_p(f, 1)), "r"(two_p(f, 2)), "r"(two_p(f, 3)), "r"(two_p(f, 4)),
+        "r"(two_p(f, 5)), "r"(two_p(f, 6)), "r"(two_p(f, 7)));
+  fe_copy(r, d);
+}
+
+// r = a - b, + 2p on a borrow: [0, 2p) for a, b < 2p.
+template <class F>
+__device__ __forceinline__ void lz_sub(uint32_t r[8], const uint32_t a[8], const uint32_t b[8], const F& f) {
+  uint32_t d[8], bw;
+  asm("sub.cc.u32 %0, %9, %17;\n\t"
+      "subc.cc.u32 %1, %10, %18;\n\t"
+      "subc.cc.u32 %2, %11, %19;\n\t"
+      "subc.cc.u32 %3, %12, %20;\n\t"
+      "subc.cc.u32 %4, %13, %21;\n\t"
+      "subc.cc.u32 %5, %14, %22;\n\t"
+      "subc.cc.u32 %6, %15, %23;\n\t"
+      "subc.cc.u32 %7, %16, %24;\n\t"
+      "subc.u32 %8, 0, 0;"
+      : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]), "=r"(bw)
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]),
+        "r"(b[0]), "r"(b[1]), "r"(b[2]), "r"(b[3]), "r"(b[4]), "r"(b[5]), "r"(b[6]), "r"(b[7]));
+  asm("add.cc.u32 %0, %0, %8;\n\t"
+      "addc.cc.u32 %1, %1, %9;\n\t"
+      "addc.cc.u32 %2, %2, %10;\n\t"
+      "addc.cc.u32 %3, %3, %11;\n\t"
+      "addc.cc.u32 %4, %4, %12;\n\t"
+      "addc.cc.u32 %5, %5, %13;\n\t"
+      "addc.cc.u32 %6, %6, %14;\n\t"
+      "addc.u32 %7, %7, %15;"
+      : "+r"(d[0]), "+r"(d[1]), "+r"(d[2]), "+r"(d[3]), "+r"(d[4]), "+r"(d[5]), "+r"(d[6]), "+r"(d[7])
+      : "r"(two_p(f, 0) & bw), "r"(two_p(f, 1) & bw), "r"(two_p(f, 2) & bw), "r"(two_p(f, 3) & bw),
+        "r"(two_p(f, 4) & bw), "r"(two_p(f, 5) & bw), "r"(two_p(f, 6) & bw), "r"(two_p(f, 7) & bw));
+  fe_copy(r, d);
+}
+
+template <class F, int kThreads = kNttThreads, int kMinBlocks = 1, bool kLazy = false>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) k_ntt_pass_tma(F f, const NttPass a, const TmaPass tp,
                                                                       const __grid_constant__ CUtensorMap tmap) {
   extern __shared__ __align__(1024) unsigned char smem_raw_tma[];
@@ -603,6 +710,20 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_ntt_pass_tma(F f, cons
   uint64_t* tw = reinterpret_cast<uint64_t*>(smem_tma + (size_t)nbuf * 2 * plane);
   uint64_t* bars = tw + 4 * (R >> 1);
   const int tid = threadIdx.x;
+  // butterfly arithmetic: canonical, or lazy (values in [0, 2p) between rounds)
+  auto bf_add = [&](uint32_t r[8], const uint32_t x[8], const uint32_t y[8]) {
+    if (kLazy) lz_add(r, x, y, f); else fe_add(r, x, y, f);
+  };
+  // a difference that a product by a twiddle follows (open: any value below 4p)
+  auto bf_sub_mul = [&](uint32_t r[8], const uint32_t x[8], const uint32_t y[8]) {
+    if (kLazy) lz_sub_open(r, x, y, f); else fe_sub(r, x, y, f);
+  };
+  auto bf_sub = [&](uint32_t r[8], const uint32_t x[8], const uint32_t y[8]) {
+    if (kLazy) lz_sub(r, x, y, f); else fe_sub(r, x, y, f);
+  };
+  auto bf_mul = [&](uint32_t r[8], const uint32_t x[8], const uint32_t w[8]) {
+    if (kLazy) fe_mul_open(r, x, w, f); else fe_mul(r, x, w, f);
+  };
 
   for (int j = tid; j < (R >> 1); j += blockDim.x) {
     uint32_t w[8];
@@ -692,7 +813,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_ntt_pass_tma(F f, cons
         fe_load_nc(hi2, a.g_hi + 4 * ((uint64_t)pos >> a.gs));
         fe_mul(g, g, hi2, f);
       }
-      fe_mul(x, x, g, f);
+      bf_mul(x, x, g);
     };
 
     // ---- decimation in frequency ----
@@ -717,12 +838,14 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_ntt_pass_tma(F f, cons
           scale_in(x0, c, q);
           scale_in(x1, c, q + h);
         }
-        fe_add(t, x0, x1, f);
-        fe_sub(x1, x0, x1, f);
+        bf_add(t, x0, x1);
         if (st > 0) {
           uint32_t w[8];
+          bf_sub_mul(x1, x0, x1);
           fe_load(w, tw + 4 * q);  // w_R^q
-          fe_mul(x1, x1, w, f);
+          bf_mul(x1, x1, w);
+        } else {
+          bf_sub(x1, x0, x1);
         }
         plane_store(lo, hi, i0, t);
         plane_store(lo, hi, i1, x1);
@@ -758,29 +881,29 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_ntt_pass_tma(F f, cons
           scale_in(x3, c, i0 + 3 * h);
         }
         // half-span 2h: (x0, x2) with w_4h^jj, (x1, x3) with w_4h^(jj + h)
-        fe_add(t, x0, x2, f);
-        fe_sub(x2, x0, x2, f);
+        bf_add(t, x0, x2);
+        if (st > 0) bf_sub_mul(x2, x0, x2); else bf_sub(x2, x0, x2);
         fe_copy(x0, t);
-        fe_add(t, x1, x3, f);
-        fe_sub(x3, x1, x3, f);
+        bf_add(t, x1, x3);
+        bf_sub_mul(x3, x1, x3);
         fe_copy(x1, t);
         if (st > 0) {
           fe_load(w, tw + 4 * (jj << (lr - 2 - st)));
-          fe_mul(x2, x2, w, f);
+          bf_mul(x2, x2, w);
         }
         fe_load(w, tw + 4 * ((jj + h) << (lr - 2 - st)));
-        fe_mul(x3, x3, w, f);
+        bf_mul(x3, x3, w);
         // half-span h: (x0, x1) and (x2, x3) with w_2h^jj
-        fe_add(t, x0, x1, f);
-        fe_sub(x1, x0, x1, f);
+        bf_add(t, x0, x1);
+        if (st > 0) bf_sub_mul(x1, x0, x1); else bf_sub(x1, x0, x1);
         fe_copy(x0, t);
-        fe_add(t, x2, x3, f);
-        fe_sub(x3, x2, x3, f);
+        bf_add(t, x2, x3);
+        if (st > 0) bf_sub_mul(x3, x2, x3); else bf_sub(x3, x2, x3);
         fe_copy(x2, t);
         if (st > 0) {
           fe_load(w, tw + 4 * (jj << (lr - 1 - st)));
-          fe_mul(x1, x1, w, f);
-          fe_mul(x3, x3, w, f);
+          bf_mul(x1, x1, w);
+          bf_mul(x3, x3, w);
         }
         plane_store(lo, hi, pidx(c, i0), x0);
         plane_store(lo, hi, pidx(c, i0 + h), x1);
@@ -815,7 +938,9 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_ntt_pass_tma(F f, cons
           } else {
             root_power<false>(w, a, e, f);
           }
-          fe_mul(x, x, w, f);
+          fe_mul(x, x, w, f);  // canonical for x < 2p as well
+        } else if (kLazy) {
+          fe_reduce_once(x, f);
         }
         fe_store(a.out + 4 * (o * B + (int64_t)k * S + jp), x);
       } else {
@@ -836,6 +961,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_ntt_pass_tma(F f, cons
             fe_load_nc(sc, a.scale);
           }
           fe_mul(x, x, sc, f);
+        } else if (kLazy) {
+          fe_reduce_once(x, f);
         }
         fe_store(a.out + 4 * outidx, x);
       }
@@ -1311,7 +1438,12 @@ static int launch_pass_tma(const F& f, const PassLaunch& L, int64_t n, int P, in
   const size_t smem = (size_t)tp.nbuf * 2 * plane + rest;
   // 128-thread blocks may take a register cap for 5 or 6 blocks per SM ("ntt.tma_blocks_per_sm")
   const int cap = L.threads == 128 ? tune_get("ntt.tma_blocks_per_sm") : 0;
-  auto kern = cap == 6 ? k_ntt_pass_tma<F, 128, 6> : cap == 5 ? k_ntt_pass_tma<F, 128, 5> : k_ntt_pass_tma<F>;
+  // lazy reduction between the rounds ("ntt.lazy") needs p < 2^254 (true of BN254's fields)
+  const bool lazy = tune_get("ntt.lazy") != 0 && (f.p(7) >> 30) == 0;
+  auto kern = cap == 6  ? k_ntt_pass_tma<F, 128, 6>
+              : cap == 5 ? k_ntt_pass_tma<F, 128, 5>
+              : lazy     ? k_ntt_pass_tma<F, kNttThreads, 1, true>
+                         : k_ntt_pass_tma<F>;
   ZKB_TRY(check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                      "NTT pass shared memory attribute"));
   int per_sm = 0;

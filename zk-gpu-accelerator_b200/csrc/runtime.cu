@@ -37,6 +37,7 @@ static Knob g_knobs[] = {
     {"ntt.full_table_mb", 4096, 0, 65536},   // budget of expanded NTT tables (MiB; 0 = two-level only)
     {"ntt.batch_spin_limit", 0, 0, 1 << 30},  // polls before a batch tile's dependency wait gives up (0 = 2^22)
     {"ntt.tma", 1, 0, 1},                    // multi-pass transforms: TMA-fed persistent passes (1) or per-thread gathers (0)
+    {"ntt.lazy", 1, 0, 1},                   // TMA passes: values in [0, 2p) between butterfly rounds (p < 2^254)
     {"ntt.tma_grid", 1, 0, 1},               // TMA passes: one persistent wave (0) or one tile per block (1)
     {"ntt.tma_blocks_per_sm", 0, 0, 6},      // TMA passes of 128-thread blocks: registers capped for 5 or 6 blocks (0 = no cap)
     {"ntt64.first_col_log", -1, -1, 6},      // int64 NTT first pass: log2 of input words per row (-1 = by size)
