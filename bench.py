@@ -584,15 +584,18 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     # torch keeps freed blocks per stream, and a leg that allocates on its own streams cannot
     # reuse them, so the cache of earlier legs would only push it into failed allocations and
     # the full synchronisations that release the cache (outside every timed region).
+    # The batched, served and int64 forms are one-GPU forms: measured at N = 1 only, so a
+    # multi-GPU run holds its GPUs for the step, the end-to-end form and the split legs.
+    single = world == 1
     batched = served = None
-    if args.workload == "large" and not args.skip_batched:
+    if single and args.workload == "large" and not args.skip_batched:
         release_cached_memory()
         batched = run_batched()
-    if args.workload == "large" and not args.skip_served:
+    if single and args.workload == "large" and not args.skip_served:
         release_cached_memory()
         served = run_served()
     int64 = None
-    if args.workload == "large" and not args.skip_int64:
+    if single and args.workload == "large" and not args.skip_int64:
         release_cached_memory()
         int64 = run_int64(cpu=rank == 0 and not args.skip_cpu_baseline)
 
@@ -600,11 +603,13 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     if world > 1:
         sharded = run_sharded(args, step, dist, device, rank, world, log_msm, log_ntt)
 
+    # the CPU baseline and the full-size parity check: rank 0 at N = 1 (every rank computes the
+    # same step, and its SHA-256 is on the line at every N)
     cpu = None
-    if rank == 0 and not args.skip_cpu_baseline:
+    if single and rank == 0 and not args.skip_cpu_baseline:
         cpu = cpu_baseline_sample(step, threads=1)
     parity = None
-    if rank == 0 and not args.skip_parity:
+    if single and rank == 0 and not args.skip_parity:
         parity = full_size_parity(step, plan_outs, digest)
 
     if dist is not None:
