@@ -5,8 +5,8 @@
 // 128-byte tensor map from global into shared memory without the issuing
 // threads touching the data; the copy reports its bytes to an mbarrier, whose
 // phase completes when the expected byte count has arrived. Only this GPU's
-// own memory is ever described by these maps, and no load here uses cluster
-// multicast.
+// own memory is ever described by these maps, and every load here lands in the
+// issuing CTA's own shared memory only.
 //
 // Alignment rules the callers keep: the global base address 16-byte aligned,
 // every stride a multiple of 16 bytes, the box's inner extent a multiple of
