@@ -93,3 +93,36 @@ def test_served_jobs_equal_the_same_jobs_alone(bases):
     s = summarize(recs)
     assert s["p99_ms"] >= s["p50_ms"] > 0
     assert server.ticks >= 4 and server.launches > 0
+
+
+def test_many_jobs_admitted_at_once_upload_in_groups(bases):
+    """30 jobs queued at once: one tick admits them all, so their rows go up in two copy groups
+    (21 + 9 jobs, each group's work waiting only for its own copies); a second server on the same
+    streams then reuses the memory the first one freed. Every job equals the same job alone."""
+    import torch
+
+    pool = [synthetic_request(60 + k, m) for k, m in enumerate([1 << 12, 1 << 13, 1 << 12, 1 << 14])]
+    alone = []
+    for r in pool:
+        job = ProofJob(r, bases)
+        prove_plain(job)
+        torch.cuda.synchronize()
+        alone.append((job.h_plain.cpu().numpy().copy(), job.msm_points()))
+    reqs = [pool[k % len(pool)] for k in range(30)]
+    for _ in range(2):
+        server = Server(bases, hbm_budget=60 << 30)
+        keep = {}
+        orig_collect = server._collect
+
+        def collect(block, server=server, keep=keep, orig=orig_collect):
+            for job_id, job in list(server.jobs.items()):
+                keep[job_id] = job
+            orig(block)
+
+        server._collect = collect
+        recs = server.run(reqs, [0.0] * len(reqs))
+        assert len(recs) == len(reqs) and len(keep) == len(reqs)
+        for job_id, job in keep.items():
+            want_h, want_pts = alone[job_id % len(pool)]
+            assert np.array_equal(job.h_plain.cpu().numpy(), want_h), job_id
+            assert job.msm_points() == want_pts, job_id
