@@ -339,254 +339,6 @@ __device__ __forceinline__ void root_power(uint32_t r[8], const NttPass& a, uint
   ntt_mul<kShared>(r, lo, hi, f);
 }
 
-// One tile (CTA-sized piece) `bid` of pass a. kFresh: the pass reads rows
-// that other CTAs wrote earlier in the same kernel (the batched form), so its
-// row loads bypass L1.
-template <class F, bool kFresh, bool kShared>
-__device__ __forceinline__ void ntt_tile(const F& f, const NttPass& a, int64_t bid,
-                                         uint64_t* sm) {
-  const int lr = a.lr, lc = a.lc;
-  const int R = 1 << lr, C = 1 << lc;
-  const int total = C << lr;
-  const int64_t S = 1ll << a.ls;
-  const int64_t B = (int64_t)R << a.ls;
-
-  // Column bases.
-  //   non-last: o = bid / (S / C), first inner index j0 = (bid % (S / C)) * C,
-  //             element (c, j) at position o B + j S + j0 + c.
-  //   last:     k2 = bid % R2, k1_0 = (bid / R2) C; row o_c = (k1_0 + c) R2 + k2,
-  //             element (c, j) at position o_c R + j.
-  int64_t o = 0, j0 = 0, k2 = 0, k1_0 = 0;
-  if (!a.last) {
-    const int64_t groups = S >> lc;
-    o = bid / groups;
-    j0 = (bid % groups) << lc;
-  } else {
-    const int64_t R2 = 1ll << a.lR2;
-    k2 = bid & (R2 - 1);
-    k1_0 = (bid >> a.lR2) << lc;
-  }
-
-  // The stage table w_R^j (j < R/2) sits in shared memory after the columns.
-  uint64_t* tw = sm + (size_t)C * ((4 << lr) + 2);
-  for (int j = threadIdx.x; j < (R >> 1); j += blockDim.x) {
-    uint32_t w[8];
-    fe_load_nc(w, a.w + 4 * ((int64_t)j << (a.log_rmax - lr)));
-    fe_store(tw + 4 * j, w);
-  }
-
-  // ---- load, with the coset pre-scale: shared position jr holds input row
-  // brev(jr), so the bit reversal happens in the global gather and the
-  // shared-memory stores stay consecutive (no bank conflicts) ----
-  for (int t = threadIdx.x; t < total; t += blockDim.x) {
-    int c, jr;
-    if (!a.last) {
-      c = t & (C - 1);
-      jr = t >> lc;
-    } else {
-      c = t >> lr;
-      jr = t & (R - 1);
-    }
-    const int j = lr ? (int)(__brev((unsigned)jr) >> (32 - lr)) : 0;
-    const int64_t pos = !a.last ? o * B + (int64_t)j * S + j0 + c
-                                : (((k1_0 + c) << a.lR2) + k2) * R + j;
-    uint32_t x[8];
-    if (kFresh && !a.first) {
-      fe_load_cg(x, a.in + 4 * pos);
-    } else {
-      fe_load_nc(x, a.in + 4 * pos);
-    }
-    if (a.first && a.g_lo && !a.inverse) {
-      uint32_t lo[8];
-      if (a.g_full) {
-        fe_load_nc(lo, a.g_full + 4 * pos);
-      } else {
-        const uint64_t m = (1ull << a.gs) - 1;
-        uint32_t hi[8];
-        fe_load_nc(lo, a.g_lo + 4 * ((uint64_t)pos & m));
-        fe_load_nc(hi, a.g_hi + 4 * ((uint64_t)pos >> a.gs));
-        ntt_mul<kShared>(lo, lo, hi, f);
-      }
-      ntt_mul<kShared>(x, x, lo, f);
-    }
-    fe_store(sm + sm_index(c, jr, lr), x);
-  }
-  __syncthreads();
-
-  // ---- DIT stages in shared memory, two per round trip (radix 4) ----
-  // A unit holds rows i0, i0 + h, i0 + 2h, i0 + 3h (h = 2^st, i0 = g 4h + jj):
-  // stage st pairs (i0, i0 + h) and (i0 + 2h, i0 + 3h) with w_2h^jj; stage
-  // st + 1 pairs (i0, i0 + 2h) with w_4h^jj and (i0 + h, i0 + 3h) with
-  // w_4h^(jj + h). In the first round jj = 0, so only w_4 multiplies.
-  int st = 0;
-  for (; st + 1 < lr; st += 2) {
-    const int h = 1 << st;
-    const int units = total >> 2;
-    for (int u = threadIdx.x; u < units; u += blockDim.x) {
-      const int c = u >> (lr - 2);
-      const int q = u & ((R >> 2) - 1);
-      const int jj = q & (h - 1);
-      const int i0 = ((q >> st) << (st + 2)) | jj;
-      uint32_t x0[8], x1[8], x2[8], x3[8], w[8], t[8];
-      fe_load(x0, sm + sm_index(c, i0, lr));
-      fe_load(x1, sm + sm_index(c, i0 + h, lr));
-      fe_load(x2, sm + sm_index(c, i0 + 2 * h, lr));
-      fe_load(x3, sm + sm_index(c, i0 + 3 * h, lr));
-      if (st > 0) {
-        fe_load(w, tw + 4 * (jj << (lr - 1 - st)));  // w_2h^jj
-        ntt_mul<kShared>(x1, x1, w, f);
-        ntt_mul<kShared>(x3, x3, w, f);
-      }
-      fe_add(t, x0, x1, f);
-      fe_sub(x1, x0, x1, f);
-      fe_copy(x0, t);
-      fe_add(t, x2, x3, f);
-      fe_sub(x3, x2, x3, f);
-      fe_copy(x2, t);
-      if (st > 0) {
-        fe_load(w, tw + 4 * (jj << (lr - 2 - st)));  // w_4h^jj
-        ntt_mul<kShared>(x2, x2, w, f);
-      }
-      fe_load(w, tw + 4 * ((jj + h) << (lr - 2 - st)));  // w_4h^(jj + h)
-      ntt_mul<kShared>(x3, x3, w, f);
-      fe_add(t, x0, x2, f);
-      fe_sub(x2, x0, x2, f);
-      fe_store(sm + sm_index(c, i0, lr), t);
-      fe_store(sm + sm_index(c, i0 + 2 * h, lr), x2);
-      fe_add(t, x1, x3, f);
-      fe_sub(x3, x1, x3, f);
-      fe_store(sm + sm_index(c, i0 + h, lr), t);
-      fe_store(sm + sm_index(c, i0 + 3 * h, lr), x3);
-    }
-    __syncthreads();
-  }
-  if (st < lr) {  // an odd number of stages: one radix-2 stage left
-    const int h = 1 << st;
-    const int half_total = total >> 1;
-    for (int b = threadIdx.x; b < half_total; b += blockDim.x) {
-      const int c = b >> (lr - 1);
-      const int k = b & ((R >> 1) - 1);
-      const int jj = k & (h - 1);
-      const int i0 = ((k >> st) << (st + 1)) | jj;
-      uint32_t u[8], v[8], w[8], x[8];
-      fe_load(u, sm + sm_index(c, i0, lr));
-      fe_load(v, sm + sm_index(c, i0 + h, lr));
-      if (st > 0) {
-        fe_load(w, tw + 4 * (jj << (lr - 1 - st)));
-        ntt_mul<kShared>(v, v, w, f);
-      }
-      fe_add(x, u, v, f);
-      fe_sub(v, u, v, f);
-      fe_store(sm + sm_index(c, i0, lr), x);
-      fe_store(sm + sm_index(c, i0 + h, lr), v);
-    }
-    __syncthreads();
-  }
-
-  // ---- store, with the pass twiddle or the final scaling ----
-  for (int t = threadIdx.x; t < total; t += blockDim.x) {
-    const int c = t & (C - 1);
-    const int k = t >> lc;
-    uint32_t x[8];
-    fe_load(x, sm + sm_index(c, k, lr));
-    if (!a.last) {
-      // w_B^((j0 + c) k) = w_N^((j0 + c) k N / B); inverse uses w_N^-e = w_N^(N - e)
-      const int64_t jp = j0 + c;
-      uint64_t e = ((uint64_t)(jp * k)) << (a.log_N - (lr + a.ls));
-      if (a.inverse && e) e = (1ull << a.log_N) - e;
-      if (e) {
-        uint32_t tw[8];
-        if (a.t_full) {
-          fe_load_nc(tw, a.t_full + 4 * (((int64_t)k << a.ls) + jp));
-        } else {
-          root_power<kShared>(tw, a, e, f);
-        }
-        ntt_mul<kShared>(x, x, tw, f);
-      }
-      const int64_t pos = o * B + (int64_t)k * S + jp;
-      fe_store(a.out + 4 * pos, x);
-    } else {
-      const int64_t oc = ((k1_0 + c) << a.lR2) + k2;
-      const int64_t outidx = (oc >> a.lR2) + ((oc & ((1ll << a.lR2) - 1)) << a.lR1) +
-                             ((int64_t)k << (a.log_n - lr));
-      if (a.inverse) {
-        uint32_t sc[8];
-        if (a.g_full) {
-          fe_load_nc(sc, a.g_full + 4 * outidx);
-        } else if (a.g_lo) {
-          const uint64_t m = (1ull << a.gs) - 1;
-          uint32_t lo[8], hi[8];
-          fe_load_nc(lo, a.g_lo + 4 * ((uint64_t)outidx & m));
-          fe_load_nc(hi, a.g_hi + 4 * ((uint64_t)outidx >> a.gs));
-          ntt_mul<kShared>(sc, lo, hi, f);
-        } else {
-          fe_load_nc(sc, a.scale);
-        }
-        ntt_mul<kShared>(x, x, sc, f);
-      }
-      fe_store(a.out + 4 * outidx, x);
-    }
-  }
-}
-
-template <class F, bool kShared>
-__global__ void __launch_bounds__(kNttThreads, 1) k_ntt_pass(F f, NttPass a) {
-  extern __shared__ uint4 smem_raw[];
-  ntt_tile<F, false, kShared>(f, a, blockIdx.x, reinterpret_cast<uint64_t*>(smem_raw));
-}
-
-// ---------------------------------------------------------------------------
-// The pass kernel fed by TMA (the default for transforms of two or more passes)
-// ---------------------------------------------------------------------------
-//
-// Each CTA takes tiles blockIdx.x, blockIdx.x + gridDim.x, ...: by default one
-// tile per CTA (a grid of all tiles), or one persistent wave ("ntt.tma_grid" =
-// 0). One thread issues the tile's tensor loads (cp.async.bulk.tensor) into a
-// shared-memory buffer and the copies complete on that buffer's mbarrier; in
-// the persistent form two buffers let the loads of the CTA's next tile run
-// while this tile computes.
-// A tile is C columns of R rows in natural order, split into two planes of
-// 16-byte half-elements (the low and the high 16 bytes of each 32-byte row),
-// so that consecutive rows read by consecutive lanes fall into distinct banks.
-// Two box loads per plane cover it (the low halves at word 0, the high halves
-// at word 2 of each row: both innermost coordinates are multiples of 16 bytes).
-//
-// The butterflies run decimation in frequency (natural order in, bit-reversed
-// order out): radix-4 rounds from the largest span down, after a radix-2 stage
-// when log2 R is odd. The first round applies the coset pre-scale as it reads
-// its rows. The store phase reads position p and writes it as frequency
-// k = brev(p), with the pass twiddle or the final scaling, as ntt_tile does.
-//
-// Plane layouts, as the boxes land: a non-last pass holds element (c, j) at
-// index j C + c (a box row is C neighbouring columns), the last pass at
-// c R + j (a box row is R neighbouring rows of one column). Lanes walk the
-// index that is contiguous, so each warp's accesses to a plane are
-// consecutive 16-byte words wherever the butterfly span allows.
-
-static constexpr uint32_t kTmaWaitLimit = 1u << 24;  // polls before a tile wait gives up
-static constexpr int kTmaBoxRows = 256;              // a TMA box extent is at most 256
-
-// Tiles whose TMA wait gave up (each such CTA stops early: its outputs are incomplete).
-__device__ unsigned g_ntt_tma_timeouts = 0;
-
-struct TmaPass {
-  int64_t ntiles;
-  int nbuf;       // 2: the next tile's loads overlap this tile's work; 1: one buffer
-  int four_d;     // the tensor map has four dimensions (else three: a last pass of a two-pass plan)
-};
-
-template <class F>
-__device__ __forceinline__ void plane_load(uint32_t x[8], const uint4* lo, const uint4* hi, int i) {
-  const uint4 l = lo[i], h = hi[i];
-  x[0] = l.x; x[1] = l.y; x[2] = l.z; x[3] = l.w;
-  x[4] = h.x; x[5] = h.y; x[6] = h.z; x[7] = h.w;
-}
-
-__device__ __forceinline__ void plane_store(uint4* lo, uint4* hi, int i, const uint32_t x[8]) {
-  lo[i] = make_uint4(x[0], x[1], x[2], x[3]);
-  hi[i] = make_uint4(x[4], x[5], x[6], x[7]);
-}
-
 // ---- lazy reduction inside a pass (moduli below 2^254) ----------------------
 // Between the butterfly rounds of a pass, values may lie anywhere in [0, 2p)
 // instead of [0, p): a difference becomes a - b + 2p, in (0, 4p), with no
@@ -692,6 +444,288 @@ __device__ __forceinline__ void lz_sub(uint32_t r[8], const uint32_t a[8], const
       : "r"(two_p(f, 0) & bw), "r"(two_p(f, 1) & bw), "r"(two_p(f, 2) & bw), "r"(two_p(f, 3) & bw),
         "r"(two_p(f, 4) & bw), "r"(two_p(f, 5) & bw), "r"(two_p(f, 6) & bw), "r"(two_p(f, 7) & bw));
   fe_copy(r, d);
+}
+
+// Fields whose modulus is known below 2^254 at compile time: BN254's Fr and Fq.
+template <class F>
+struct LazyOk {
+  static constexpr bool value = false;
+};
+template <>
+struct LazyOk<FrP> {
+  static constexpr bool value = true;
+};
+template <>
+struct LazyOk<FqP> {
+  static constexpr bool value = true;
+};
+
+// One tile (CTA-sized piece) `bid` of pass a. kFresh: the pass reads rows
+// that other CTAs wrote earlier in the same kernel (the batched form), so its
+// row loads bypass L1.
+template <class F, bool kFresh, bool kShared>
+__device__ __forceinline__ void ntt_tile(const F& f, const NttPass& a, int64_t bid,
+                                         uint64_t* sm) {
+  const int lr = a.lr, lc = a.lc;
+  const int R = 1 << lr, C = 1 << lc;
+  const int total = C << lr;
+  // lazy reduction between the rounds (inline products, BN254's fields): values in [0, 2p),
+  // canonical again at the store
+  constexpr bool kLz = !kShared && LazyOk<F>::value;
+  auto mul_l = [&](uint32_t r[8], const uint32_t x[8], const uint32_t w[8]) {
+    if (kLz) fe_mul_open(r, x, w, f); else ntt_mul<kShared>(r, x, w, f);
+  };
+  auto add_l = [&](uint32_t r[8], const uint32_t x[8], const uint32_t y[8]) {
+    if (kLz) lz_add(r, x, y, f); else fe_add(r, x, y, f);
+  };
+  auto sub_l = [&](uint32_t r[8], const uint32_t x[8], const uint32_t y[8]) {
+    if (kLz) lz_sub(r, x, y, f); else fe_sub(r, x, y, f);
+  };
+  // a difference that a product by a twiddle follows
+  auto sub_mul_l = [&](uint32_t r[8], const uint32_t x[8], const uint32_t y[8]) {
+    if (kLz) lz_sub_open(r, x, y, f); else fe_sub(r, x, y, f);
+  };
+  const int64_t S = 1ll << a.ls;
+  const int64_t B = (int64_t)R << a.ls;
+
+  // Column bases.
+  //   non-last: o = bid / (S / C), first inner index j0 = (bid % (S / C)) * C,
+  //             element (c, j) at position o B + j S + j0 + c.
+  //   last:     k2 = bid % R2, k1_0 = (bid / R2) C; row o_c = (k1_0 + c) R2 + k2,
+  //             element (c, j) at position o_c R + j.
+  int64_t o = 0, j0 = 0, k2 = 0, k1_0 = 0;
+  if (!a.last) {
+    const int64_t groups = S >> lc;
+    o = bid / groups;
+    j0 = (bid % groups) << lc;
+  } else {
+    const int64_t R2 = 1ll << a.lR2;
+    k2 = bid & (R2 - 1);
+    k1_0 = (bid >> a.lR2) << lc;
+  }
+
+  // The stage table w_R^j (j < R/2) sits in shared memory after the columns.
+  uint64_t* tw = sm + (size_t)C * ((4 << lr) + 2);
+  for (int j = threadIdx.x; j < (R >> 1); j += blockDim.x) {
+    uint32_t w[8];
+    fe_load_nc(w, a.w + 4 * ((int64_t)j << (a.log_rmax - lr)));
+    fe_store(tw + 4 * j, w);
+  }
+
+  // ---- load, with the coset pre-scale: shared position jr holds input row
+  // brev(jr), so the bit reversal happens in the global gather and the
+  // shared-memory stores stay consecutive (no bank conflicts) ----
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    int c, jr;
+    if (!a.last) {
+      c = t & (C - 1);
+      jr = t >> lc;
+    } else {
+      c = t >> lr;
+      jr = t & (R - 1);
+    }
+    const int j = lr ? (int)(__brev((unsigned)jr) >> (32 - lr)) : 0;
+    const int64_t pos = !a.last ? o * B + (int64_t)j * S + j0 + c
+                                : (((k1_0 + c) << a.lR2) + k2) * R + j;
+    uint32_t x[8];
+    if (kFresh && !a.first) {
+      fe_load_cg(x, a.in + 4 * pos);
+    } else {
+      fe_load_nc(x, a.in + 4 * pos);
+    }
+    if (a.first && a.g_lo && !a.inverse) {
+      uint32_t lo[8];
+      if (a.g_full) {
+        fe_load_nc(lo, a.g_full + 4 * pos);
+      } else {
+        const uint64_t m = (1ull << a.gs) - 1;
+        uint32_t hi[8];
+        fe_load_nc(lo, a.g_lo + 4 * ((uint64_t)pos & m));
+        fe_load_nc(hi, a.g_hi + 4 * ((uint64_t)pos >> a.gs));
+        ntt_mul<kShared>(lo, lo, hi, f);
+      }
+      mul_l(x, x, lo);
+    }
+    fe_store(sm + sm_index(c, jr, lr), x);
+  }
+  __syncthreads();
+
+  // ---- DIT stages in shared memory, two per round trip (radix 4) ----
+  // A unit holds rows i0, i0 + h, i0 + 2h, i0 + 3h (h = 2^st, i0 = g 4h + jj):
+  // stage st pairs (i0, i0 + h) and (i0 + 2h, i0 + 3h) with w_2h^jj; stage
+  // st + 1 pairs (i0, i0 + 2h) with w_4h^jj and (i0 + h, i0 + 3h) with
+  // w_4h^(jj + h). In the first round jj = 0, so only w_4 multiplies.
+  int st = 0;
+  for (; st + 1 < lr; st += 2) {
+    const int h = 1 << st;
+    const int units = total >> 2;
+    for (int u = threadIdx.x; u < units; u += blockDim.x) {
+      const int c = u >> (lr - 2);
+      const int q = u & ((R >> 2) - 1);
+      const int jj = q & (h - 1);
+      const int i0 = ((q >> st) << (st + 2)) | jj;
+      uint32_t x0[8], x1[8], x2[8], x3[8], w[8], t[8];
+      fe_load(x0, sm + sm_index(c, i0, lr));
+      fe_load(x1, sm + sm_index(c, i0 + h, lr));
+      fe_load(x2, sm + sm_index(c, i0 + 2 * h, lr));
+      fe_load(x3, sm + sm_index(c, i0 + 3 * h, lr));
+      if (st > 0) {
+        fe_load(w, tw + 4 * (jj << (lr - 1 - st)));  // w_2h^jj
+        mul_l(x1, x1, w);
+        mul_l(x3, x3, w);
+      }
+      add_l(t, x0, x1);
+      sub_l(x1, x0, x1);
+      fe_copy(x0, t);
+      add_l(t, x2, x3);
+      sub_mul_l(x3, x2, x3);  // multiplied below in every round
+      fe_copy(x2, t);
+      if (st > 0) {
+        fe_load(w, tw + 4 * (jj << (lr - 2 - st)));  // w_4h^jj
+        mul_l(x2, x2, w);
+      }
+      fe_load(w, tw + 4 * ((jj + h) << (lr - 2 - st)));  // w_4h^(jj + h)
+      mul_l(x3, x3, w);
+      add_l(t, x0, x2);
+      sub_l(x2, x0, x2);
+      fe_store(sm + sm_index(c, i0, lr), t);
+      fe_store(sm + sm_index(c, i0 + 2 * h, lr), x2);
+      add_l(t, x1, x3);
+      sub_l(x3, x1, x3);
+      fe_store(sm + sm_index(c, i0 + h, lr), t);
+      fe_store(sm + sm_index(c, i0 + 3 * h, lr), x3);
+    }
+    __syncthreads();
+  }
+  if (st < lr) {  // an odd number of stages: one radix-2 stage left
+    const int h = 1 << st;
+    const int half_total = total >> 1;
+    for (int b = threadIdx.x; b < half_total; b += blockDim.x) {
+      const int c = b >> (lr - 1);
+      const int k = b & ((R >> 1) - 1);
+      const int jj = k & (h - 1);
+      const int i0 = ((k >> st) << (st + 1)) | jj;
+      uint32_t u[8], v[8], w[8], x[8];
+      fe_load(u, sm + sm_index(c, i0, lr));
+      fe_load(v, sm + sm_index(c, i0 + h, lr));
+      if (st > 0) {
+        fe_load(w, tw + 4 * (jj << (lr - 1 - st)));
+        mul_l(v, v, w);
+      }
+      add_l(x, u, v);
+      sub_l(v, u, v);
+      fe_store(sm + sm_index(c, i0, lr), x);
+      fe_store(sm + sm_index(c, i0 + h, lr), v);
+    }
+    __syncthreads();
+  }
+
+  // ---- store, with the pass twiddle or the final scaling ----
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    const int c = t & (C - 1);
+    const int k = t >> lc;
+    uint32_t x[8];
+    fe_load(x, sm + sm_index(c, k, lr));
+    if (!a.last) {
+      // w_B^((j0 + c) k) = w_N^((j0 + c) k N / B); inverse uses w_N^-e = w_N^(N - e)
+      const int64_t jp = j0 + c;
+      uint64_t e = ((uint64_t)(jp * k)) << (a.log_N - (lr + a.ls));
+      if (a.inverse && e) e = (1ull << a.log_N) - e;
+      if (e) {
+        uint32_t tw[8];
+        if (a.t_full) {
+          fe_load_nc(tw, a.t_full + 4 * (((int64_t)k << a.ls) + jp));
+        } else {
+          root_power<kShared>(tw, a, e, f);
+        }
+        ntt_mul<kShared>(x, x, tw, f);  // canonical for x < 2p as well
+      } else if (kLz) {
+        fe_reduce_once(x, f);
+      }
+      const int64_t pos = o * B + (int64_t)k * S + jp;
+      fe_store(a.out + 4 * pos, x);
+    } else {
+      const int64_t oc = ((k1_0 + c) << a.lR2) + k2;
+      const int64_t outidx = (oc >> a.lR2) + ((oc & ((1ll << a.lR2) - 1)) << a.lR1) +
+                             ((int64_t)k << (a.log_n - lr));
+      if (a.inverse) {
+        uint32_t sc[8];
+        if (a.g_full) {
+          fe_load_nc(sc, a.g_full + 4 * outidx);
+        } else if (a.g_lo) {
+          const uint64_t m = (1ull << a.gs) - 1;
+          uint32_t lo[8], hi[8];
+          fe_load_nc(lo, a.g_lo + 4 * ((uint64_t)outidx & m));
+          fe_load_nc(hi, a.g_hi + 4 * ((uint64_t)outidx >> a.gs));
+          ntt_mul<kShared>(sc, lo, hi, f);
+        } else {
+          fe_load_nc(sc, a.scale);
+        }
+        ntt_mul<kShared>(x, x, sc, f);
+      } else if (kLz) {
+        fe_reduce_once(x, f);
+      }
+      fe_store(a.out + 4 * outidx, x);
+    }
+  }
+}
+
+template <class F, bool kShared>
+__global__ void __launch_bounds__(kNttThreads, 1) k_ntt_pass(F f, NttPass a) {
+  extern __shared__ uint4 smem_raw[];
+  ntt_tile<F, false, kShared>(f, a, blockIdx.x, reinterpret_cast<uint64_t*>(smem_raw));
+}
+
+// ---------------------------------------------------------------------------
+// The pass kernel fed by TMA (the default for transforms of two or more passes)
+// ---------------------------------------------------------------------------
+//
+// Each CTA takes tiles blockIdx.x, blockIdx.x + gridDim.x, ...: by default one
+// tile per CTA (a grid of all tiles), or one persistent wave ("ntt.tma_grid" =
+// 0). One thread issues the tile's tensor loads (cp.async.bulk.tensor) into a
+// shared-memory buffer and the copies complete on that buffer's mbarrier; in
+// the persistent form two buffers let the loads of the CTA's next tile run
+// while this tile computes.
+// A tile is C columns of R rows in natural order, split into two planes of
+// 16-byte half-elements (the low and the high 16 bytes of each 32-byte row),
+// so that consecutive rows read by consecutive lanes fall into distinct banks.
+// Two box loads per plane cover it (the low halves at word 0, the high halves
+// at word 2 of each row: both innermost coordinates are multiples of 16 bytes).
+//
+// The butterflies run decimation in frequency (natural order in, bit-reversed
+// order out): radix-4 rounds from the largest span down, after a radix-2 stage
+// when log2 R is odd. The first round applies the coset pre-scale as it reads
+// its rows. The store phase reads position p and writes it as frequency
+// k = brev(p), with the pass twiddle or the final scaling, as ntt_tile does.
+//
+// Plane layouts, as the boxes land: a non-last pass holds element (c, j) at
+// index j C + c (a box row is C neighbouring columns), the last pass at
+// c R + j (a box row is R neighbouring rows of one column). Lanes walk the
+// index that is contiguous, so each warp's accesses to a plane are
+// consecutive 16-byte words wherever the butterfly span allows.
+
+static constexpr uint32_t kTmaWaitLimit = 1u << 24;  // polls before a tile wait gives up
+static constexpr int kTmaBoxRows = 256;              // a TMA box extent is at most 256
+
+// Tiles whose TMA wait gave up (each such CTA stops early: its outputs are incomplete).
+__device__ unsigned g_ntt_tma_timeouts = 0;
+
+struct TmaPass {
+  int64_t ntiles;
+  int nbuf;       // 2: the next tile's loads overlap this tile's work; 1: one buffer
+  int four_d;     // the tensor map has four dimensions (else three: a last pass of a two-pass plan)
+};
+
+template <class F>
+__device__ __forceinline__ void plane_load(uint32_t x[8], const uint4* lo, const uint4* hi, int i) {
+  const uint4 l = lo[i], h = hi[i];
+  x[0] = l.x; x[1] = l.y; x[2] = l.z; x[3] = l.w;
+  x[4] = h.x; x[5] = h.y; x[6] = h.z; x[7] = h.w;
+}
+
+__device__ __forceinline__ void plane_store(uint4* lo, uint4* hi, int i, const uint32_t x[8]) {
+  lo[i] = make_uint4(x[0], x[1], x[2], x[3]);
+  hi[i] = make_uint4(x[4], x[5], x[6], x[7]);
 }
 
 template <class F, int kThreads = kNttThreads, int kMinBlocks = 1, bool kLazy = false>
